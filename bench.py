@@ -1,0 +1,366 @@
+"""Debye pair·q throughput on B200: FP32-recurrence kernel vs plain FP64, with
+the reference's CPU Debye (its FP64 restatement) timed beside it.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload ellipsoid_solvent_100k] [--precision fp32]
+
+One step = one full six-profile Debye solve of the workload (100,000 atoms in
+an 80×40×40 Å ellipsoid, FoXS excluded volume + surface hydration, nq = 1,000
+on [0, 1] Å⁻¹ by default). `value` is pair·q/s with the coordinates resident
+in HBM (pd_plan_execute), `e2e` the same metric through the blocking C-ABI
+call with host buffers (pd_solve: plan, upload, kernels, download). Work unit:
+one unordered atom pair at one q, P = N(N-1)/2·nq per solve.
+
+With --gpus N (torchrun) every rank solves its own copy of the workload
+(replicas: per-GPU work fixed, "scaling": "weak"); the step time is the max
+over ranks and `value` is the whole-job rate. Rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "Debye pair·q evals/s (FP32 recurrence, FP64 reduction)"
+UNIT = "pair·q/s"
+# FP32 flops of one pair·q in the class-mode inner loop: recurrence step
+# (FFMA + FADD = 3) + accumulation (FFMA = 2).
+FLOPS_PER_PAIRQ = {"class": 5, "weighted": 7}
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except (FileNotFoundError, OSError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons, power = [], None, set(), []
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax = float(p[2])
+                power.append(float(p[3]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm),
+                "power_w_median": statistics.median(power) if power else None}
+
+
+def cpu_sample(w, n_sample=6000, n_q=8, threads=0):
+    """Time the FP64 oracle (the reference's Debye code restated, q-parallel
+    on host threads) on a bounded sample of the workload: the first
+    `n_sample` atoms and `n_q` grid points spread over the q range."""
+    from oracle import oracle as O
+    req = w.request
+    n = min(n_sample, req.n_atoms)
+    qi = np.unique(np.linspace(0, req.nq - 1, n_q).astype(np.int64)).astype(np.uint32)
+    xyz = (req.xyz[0] if req.xyz.ndim == 3 else req.xyz)[:n]
+    t0 = time.perf_counter()
+    if req.ff_excluded is None and req.hyd_weights is None:
+        O.vacuum(xyz, req.species[:n], req.ff_atoms, req.qmin, req.qmax, req.nq, qi, threads)
+    else:
+        O.build_model(xyz, req.species[:n], req.ff_atoms, req.ff_excluded,
+                      None if req.hyd_weights is None else req.hyd_weights[:n], req.ff_water,
+                      req.qmin, req.qmax, req.nq, qi, threads)
+    dt = time.perf_counter() - t0
+    pq = n * (n - 1) // 2 * len(qi)
+    return pq / dt, pq, dt, f"first {n} of {req.n_atoms} atoms × {len(qi)} of {req.nq} q points"
+
+
+def run_reference(args, ws, rank):
+    """The reference arm: the FP64 CPU restatement of the reference's Debye
+    path on all host cores, each step a bounded sample of the workload."""
+    if rank != 0:
+        return
+    from pripps_b200 import workloads
+    w = workloads.WORKLOADS[args.workload](args.precision)
+    cores = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        cpu_sample(w, args.cpu_atoms, args.cpu_q)
+    rates, times = [], []
+    sample = None
+    for _ in range(args.steps):
+        rate, pq, dt, sample = cpu_sample(w, args.cpu_atoms, args.cpu_q)
+        rates.append(rate)
+        times.append(dt)
+    pq_total = pq * len(times)
+    value = pq_total / sum(times)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": config_dict(args, w),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def config_dict(args, w):
+    req = w.request
+    solvent = "vacuum"
+    if req.ff_excluded is not None:
+        solvent = "foxs_fraser_excluded" + ("+surface_hydration" if req.hyd_weights is not None else "")
+    return {"workload": w.name, "n_atoms": req.n_atoms, "nq": req.nq,
+            "q_range": [req.qmin, req.qmax], "n_frames": req.n_frames, "solvent": solvent,
+            "precision_form": args.precision, "pairs_per_solve": w.pairs,
+            "pair_q_per_step": w.pair_q,
+            "l2": "flushed between timed steps (256 MiB write outside the timed events)"}
+
+
+def load_traffic(workload):
+    """DRAM bytes per pair-kernel launch from the committed ncu summary."""
+    p = ROOT / "profiles" / "traffic.json"
+    if not p.exists():
+        return None
+    try:
+        d = json.loads(p.read_text())
+        return d.get(workload, {}).get("dram_bytes_per_launch")
+    except (ValueError, OSError):
+        return None
+
+
+def run_ours(args, ws, rank, local):
+    import torch
+
+    from pripps_b200 import _lib, workloads
+    from pripps_b200.debye import solve
+
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    w = workloads.WORKLOADS[args.workload](args.precision)
+    req = w.request
+    ctx = _lib.Context(local)
+    lib = _lib.lib()
+
+    peak_ffma, peak_ffma2 = C.c_double(), C.c_double()
+    _lib.check(lib.pd_measure_fp32_peak(ctx.handle, C.byref(peak_ffma), C.byref(peak_ffma2)),
+               ctx.handle)
+
+    # ---- device-resident path
+    r = req.c_struct()
+    plan = C.c_void_p()
+    _lib.check(lib.pd_plan_create(ctx.handle, C.byref(r), C.byref(plan)), ctx.handle)
+    kb, tj, ntile, dbytes, ubytes = (C.c_uint32(), C.c_uint32(), C.c_uint64(), C.c_uint64(),
+                                     C.c_uint64())
+    lib.pd_plan_info(plan, C.byref(kb), C.byref(tj), C.byref(ntile), C.byref(dbytes),
+                     C.byref(ubytes))
+    xyz = torch.from_numpy(req.xyz).to(f"cuda:{local}")
+    out = torch.empty((6, req.nq), dtype=torch.float64, device=f"cuda:{local}")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+    stream = torch.cuda.current_stream()
+    sp = stream.cuda_stream
+
+    def execute():
+        _lib.check(lib.pd_plan_execute(ctx.handle, plan, xyz.data_ptr(), out.data_ptr(), sp),
+                   ctx.handle)
+
+    for _ in range(args.warmup):
+        execute()
+        flush.zero_()
+    torch.cuda.synchronize()
+    if ws > 1:
+        torch.distributed.barrier()
+    lib.pd_plan_set_profiling(ctx.handle, plan, 1)
+    clocks = ClockSampler(local)
+    clocks.start()
+    launches0 = ctx.launch_count()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    torch.cuda.synchronize()
+    for i in range(args.steps):
+        starts[i].record(stream)
+        execute()
+        ends[i].record(stream)
+        flush.zero_()
+    torch.cuda.synchronize()
+    launches = ctx.launch_count() - launches0
+    clk = clocks.stop()
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    total_ms = sum(step_ms)
+    pair_ms, n_pair = C.c_double(), C.c_uint64()
+    _lib.check(lib.pd_plan_pair_kernel_ms(ctx.handle, plan, C.byref(pair_ms), C.byref(n_pair)),
+               ctx.handle)
+    lib.pd_plan_set_profiling(ctx.handle, plan, 0)
+    if ws > 1:
+        t = torch.tensor([total_ms], dtype=torch.float64, device=f"cuda:{local}")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms_per_step = total_ms / args.steps
+    value = ws * w.pair_q / (ms_per_step * 1e-3)
+    result_dev = out.cpu().numpy()
+
+    # ---- plain FP64 kernel on the same structure (bounded q grid)
+    fp64 = None
+    if rank == 0 and not args.no_fp64:
+        from pripps_b200 import workloads as W
+        r64 = W.globule_request(w.globule, req.qmin, req.qmax, args.fp64_nq,
+                                req.ff_excluded is not None, "fp64")
+        p64 = C.c_void_p()
+        c64 = r64.c_struct()
+        _lib.check(lib.pd_plan_create(ctx.handle, C.byref(c64), C.byref(p64)), ctx.handle)
+        out64 = torch.empty((6, r64.nq), dtype=torch.float64, device=f"cuda:{local}")
+        _lib.check(lib.pd_plan_execute(ctx.handle, p64, xyz.data_ptr(), out64.data_ptr(), sp),
+                   ctx.handle)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        _lib.check(lib.pd_plan_execute(ctx.handle, p64, xyz.data_ptr(), out64.data_ptr(), sp),
+                   ctx.handle)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms64 = e0.elapsed_time(e1)
+        pq64 = w.pairs * r64.nq
+        lib.pd_plan_destroy(ctx.handle, p64)
+        fp64 = {"value": pq64 / (ms64 * 1e-3), "unit": UNIT, "nq": r64.nq, "ms": ms64,
+                "fp32_over_fp64": (w.pair_q / (ms_per_step * 1e-3)) / (pq64 / (ms64 * 1e-3))}
+
+    # ---- end to end through the C ABI with host buffers
+    e2e_times = []
+    res_host = None
+    for i in range(args.e2e_steps + 1):
+        t0 = time.perf_counter()
+        res_host = solve(req, ctx)
+        dt = time.perf_counter() - t0
+        if i > 0:
+            e2e_times.append(dt)
+    e2e_ms = 1e3 * sum(e2e_times) / len(e2e_times)
+    if ws > 1:
+        t = torch.tensor([e2e_ms], dtype=torch.float64, device=f"cuda:{local}")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    same = bool(np.array_equal(res_host, result_dev))
+    lib.pd_plan_destroy(ctx.handle, plan)
+
+    if rank == 0:
+        mode = "class"
+        if req.hyd_weights is not None:
+            keys = set(zip(req.species.tolist(), req.hyd_weights.tolist()))
+            mode = "weighted" if len(keys) > 48 else "class"
+        flops = FLOPS_PER_PAIRQ[mode]
+        launch_ms = pair_ms.value / max(n_pair.value, 1)
+        achieved = flops * w.pair_q / (launch_ms * 1e-3) / 1e12
+        peak = peak_ffma.value
+        cpu = None
+        if not args.no_cpu:
+            rate, pq, dt, sample = cpu_sample(w, args.cpu_atoms, args.cpu_q)
+            cpu = {"value": rate, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port",
+                   "sample": sample, "seconds": dt}
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": config_dict(args, w),
+            "e2e": {"value": ws * w.pair_q / (e2e_ms * 1e-3), "unit": UNIT,
+                    "ms_per_step": e2e_ms, "h2d_bytes_per_step": int(ubytes.value),
+                    "d2h_bytes_per_step": 6 * req.nq * 8,
+                    "same_result_as_device_path": same},
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak,
+                         "unit": "TFLOP/s", "frac": achieved / peak,
+                         "traffic": load_traffic(w.name),
+                         "kernel": "pd_pairs_fp32", "flops_per_pair_q": flops,
+                         "kernel_ms_per_launch": launch_ms,
+                         "peak_source": "measured FFMA probe (pd_measure_fp32_peak), this run",
+                         "peak_ffma2_tflops": peak_ffma2.value,
+                         "theoretical_peak_tflops_at_max_clock":
+                             2 * 128 * 148 * (clk["sm_max_mhz"] or 1965.0) * 1e-6},
+            "fp64_kernel": fp64,
+            "cpu_baseline": cpu,
+            "clocks": clk,
+            "tiles": {"q_block": kb.value, "j_chunk": tj.value, "tiles_per_solve": ntile.value,
+                      "device_bytes": dbytes.value},
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if ws > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--workload", default="ellipsoid_solvent_100k")
+    ap.add_argument("--precision", default="fp32", choices=("fp32", "fp64"))
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--fp64-nq", type=int, default=64)
+    ap.add_argument("--cpu-atoms", type=int, default=6000)
+    ap.add_argument("--cpu-q", type=int, default=8)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    ws, rank, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, ws, rank)
+    else:
+        run_ours(args, ws, rank, local)
+
+
+if __name__ == "__main__":
+    main()

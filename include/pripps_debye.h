@@ -1,0 +1,202 @@
+/*
+ * pripps_debye.h — C ABI of the B200 Debye backend (libpripps_debye.so).
+ *
+ * One backend only: every entry point runs the sum on an NVIDIA B200
+ * (sm_100a). There is no CPU fallback; without a usable device the calls
+ * return PD_ENODEV.
+ *
+ * The library computes, for one structure (or a batch of trajectory frames),
+ * the six partial Debye profiles that the reference caches per q
+ * (DebyeTerms, src/debye.rs:176-184), in this row order:
+ *
+ *   row 0  atoms               Σ_i A_i² + 2 Σ_{i<j} A_i A_j sinc(q r_ij)
+ *   row 1  excluded            same with C_i (excluded-volume dummies)
+ *   row 2  hydration           same with B_i (hydration dummies)
+ *   row 3  atom_excluded       Σ_a Σ_b A_a C_b sinc(q r_ab)   (i = j included)
+ *   row 4  atom_hydration      Σ_a Σ_b A_a B_b sinc(q r_ab)
+ *   row 5  excluded_hydration  Σ_a Σ_b C_a B_b sinc(q r_ab)
+ *
+ * on the reference's uniform grid q_k = qmin + (qmax-qmin)·k/max(nq-1, 1)
+ * (src/q_sampler.rs:24-29), with A_i = F_{s_i}(q), C_i = C_{s_i}(q) and
+ * B_i = w_i·F_H2O(q): the atom, excluded-volume and hydration scatterers all
+ * sit at the atom positions, as the reference's Fraser/FoXS excluded volume
+ * (src/solvent/fraser.rs:64-100), per-kind excluded solvent
+ * (src/solvent/per_kind_excluded.rs:16-39) and SASA hydration
+ * (src/solvent/sasa.rs:34-71) place them.
+ *
+ * Conventions: every int-returning call returns PD_OK (0) or a negative
+ * PD_E* code, and pd_last_error() describes the most recent failure of the
+ * calling thread on that context. Output buffers are caller-owned. Request
+ * inputs are copied at submission: the caller may free them once
+ * pd_submit()/pd_solve() returns. A context is internally synchronised; any
+ * host thread may use it.
+ */
+#ifndef PRIPPS_DEBYE_H
+#define PRIPPS_DEBYE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PD_ABI_VERSION 1
+
+/* ---- status codes ---- */
+#define PD_OK 0
+#define PD_EINVAL (-1)    /* malformed request: nq = 0, N = 0, NaN input, bad ids */
+#define PD_ENOMEM (-2)    /* a host or device allocation failed */
+#define PD_EBUDGET (-3)   /* the request can never fit the context's memory budget */
+#define PD_ETIMEOUT (-4)  /* pd_wait timed out, or a bounded device wait expired */
+#define PD_EDEVICE (-5)   /* a CUDA call failed (message in pd_last_error) */
+#define PD_ENOTFOUND (-6) /* unknown ticket */
+#define PD_ECANCELED (-7) /* the request was cancelled before it finished */
+#define PD_ENODEV (-8)    /* no sm_100 device at the requested ordinal */
+
+/* ---- precision forms ---- */
+#define PD_FP32_FP64RED 0 /* FP32 recurrence sinc, FP32 per-tile sums, FP64 reduction */
+#define PD_FP64 1         /* plain FP64 sinc and accumulation throughout */
+
+/* ---- output layout ---- */
+#define PD_NUM_TERMS 6 /* rows of the [6][nq] output, see above */
+
+typedef struct pd_ctx pd_ctx;
+
+/*
+ * One Debye solve. Replaces the inputs the reference's build_model gathers
+ * per q (src/debye.rs:83-101): the structure (Structure{pos, ids},
+ * src/structure.rs:27-31), the per-species form factors evaluated on the q
+ * grid (formfactor_by_index, src/formfactor.rs:528-544), the excluded-volume
+ * dummy form factors (ExcludedVolume::unit_scale_dummies,
+ * src/solvent/mod.rs:385-403) and the hydration weights plus shared water
+ * form factor (DummySet::Weighted, src/solvent/mod.rs:365-371).
+ */
+typedef struct pd_request {
+    uint64_t n_atoms;           /* N >= 1 */
+    const double *xyz;          /* [n_frames][N][3] positions in Å (AoS) */
+    const uint32_t *species;    /* [N] species ids, each < n_species */
+    uint32_t n_species;         /* S >= 1 */
+    uint32_t precision;         /* PD_FP32_FP64RED or PD_FP64 */
+    const double *ff_atoms;     /* [S][nq] F_s(q_k); required */
+    const double *ff_excluded;  /* [S][nq] C_s(q_k), or NULL: no excluded volume */
+    const double *hyd_weights;  /* [N] w_i, or NULL: no hydration */
+    const double *ff_water;     /* [nq] F_H2O(q_k); required iff hyd_weights */
+    double qmin, qmax;          /* grid ends (inclusive), qmin >= 0 */
+    uint64_t nq;                /* >= 1 */
+    uint64_t n_frames;          /* 0 or 1: one structure; > 1: trajectory batch */
+    const double *frame_weights;/* [n_frames] weights of the mean, or NULL: uniform */
+    uint32_t flags;             /* reserved, must be 0 */
+    uint32_t reserved;          /* must be 0 */
+} pd_request;
+
+/* Create a context on CUDA device `device`. `mem_budget_bytes` caps the
+ * device memory the context holds for admitted requests (0 = 90 % of the
+ * device's free memory). No reference counterpart: the reference holds no
+ * device state (its Debye path is rayon on the host, src/debye.rs:90-92). */
+int pd_ctx_create(int device, uint64_t mem_budget_bytes, pd_ctx **out);
+
+/* Release every resource of the context; outstanding tickets are cancelled. */
+void pd_ctx_destroy(pd_ctx *ctx);
+
+/* Blocking solve with host buffers: out_terms is [6][nq] (n_frames <= 1) or
+ * the frame-weighted mean Σ_f w_f·T_f / Σ_f w_f of the six profiles.
+ * Replaces the per-q body of build_model (src/debye.rs:90-130) and, for the
+ * vacuum path, QSampler::run_parallel over intensity_at_q
+ * (src/debye.rs:58-60, :200-211) — rows 1..5 are zero then — and the frame
+ * loop of trajectory_average (src/trajectory.rs:198-248; the weighted mean of
+ * the terms combines to the weighted mean of the totals because combine is
+ * linear in the terms). */
+int pd_solve(pd_ctx *ctx, const pd_request *req, double *out_terms);
+
+/* Plans: the host-side preparation of a request (atom classes, padded
+ * layout, tile list, reduction lists, uploaded form-factor tables) split from
+ * its execution, for callers that solve the same topology many times with new
+ * coordinates — trajectory frames (src/trajectory.rs:198-223) or a caller
+ * whose coordinates already live in device memory. pd_plan_create reads every
+ * pointer of `req` as HOST memory except `xyz`, which may be NULL (coordinates
+ * are supplied per execution). No reference counterpart beyond build_model
+ * (src/debye.rs:78-136), which re-derives all of this on every call. */
+typedef struct pd_plan pd_plan;
+int pd_plan_create(pd_ctx *ctx, const pd_request *req, pd_plan **out);
+
+/* Enqueue one solve of `plan` on `stream` (a cudaStream_t; NULL = legacy
+ * default stream). xyz_dev is DEVICE memory [n_frames][N][3] and
+ * out_terms_dev DEVICE memory for the [6][nq] result; both must stay valid
+ * until the stream passes this call. Executions of one plan on several
+ * streams at once race on the plan's scratch and must be serialised. */
+int pd_plan_execute(pd_ctx *ctx, pd_plan *plan, const double *xyz_dev, double *out_terms_dev,
+                    void *stream);
+
+/* Blocking execution with HOST coordinates and a HOST [6][nq] result. */
+int pd_plan_execute_host(pd_ctx *ctx, pd_plan *plan, const double *xyz_host, double *out_terms);
+
+/* q-block length, atom-chunk length, tiles per execution, device bytes held
+ * and bytes uploaded from the host when the plan is created. */
+int pd_plan_info(const pd_plan *plan, uint32_t *q_block, uint32_t *j_chunk, uint64_t *n_tiles,
+                 uint64_t *device_bytes, uint64_t *upload_bytes);
+
+/* Kernel timing: with profiling enabled every pd_plan_execute brackets its
+ * pair kernel with CUDA events on the execution stream; pd_plan_pair_kernel_ms
+ * waits for them and reports the summed duration and the number of timed
+ * launches since profiling was (re)enabled. */
+int pd_plan_set_profiling(pd_ctx *ctx, pd_plan *plan, int enable);
+int pd_plan_pair_kernel_ms(pd_ctx *ctx, pd_plan *plan, double *total_ms, uint64_t *n_launches);
+void pd_plan_destroy(pd_ctx *ctx, pd_plan *plan);
+
+/* Continuous-batching request loop. pd_submit copies the request, queues it
+ * for admission (admitted when device memory within the budget frees up) and
+ * returns a ticket at once; its tiles then run interleaved with those of the
+ * other admitted requests. pd_wait blocks up to timeout_ms (< 0: forever) and
+ * copies the [6][nq] result out; pd_poll returns 1 when the ticket finished,
+ * 0 while it is pending, or a negative code. The result of a ticket is
+ * independent of what else ran beside it (deterministic per-request
+ * reduction). pd_wait hands the result out once: it then frees it, and a
+ * second pd_wait with a non-NULL out_terms returns PD_EINVAL. */
+int pd_submit(pd_ctx *ctx, const pd_request *req, uint64_t *ticket);
+int pd_wait(pd_ctx *ctx, uint64_t ticket, int timeout_ms, double *out_terms);
+int pd_poll(pd_ctx *ctx, uint64_t ticket);
+int pd_cancel(pd_ctx *ctx, uint64_t ticket);
+
+/* Timestamps of a finished ticket in seconds on the context's monotonic
+ * clock: submission, admission to the device, completion. */
+int pd_ticket_times(pd_ctx *ctx, uint64_t ticket, double *t_submit, double *t_admit,
+                    double *t_done);
+
+/* The recombination of the six terms into I(q) (DebyeTerms::combine,
+ * src/debye.rs:187-194); total is [nq]. Host-only. */
+int pd_combine(const double *terms, uint64_t nq, double volume_scale,
+               double contrast_density, double *total);
+
+/* Message describing the last failure on this context from the calling
+ * thread ("" if none); NULL ctx gives the last context-free failure. */
+const char *pd_last_error(pd_ctx *ctx);
+
+/* Kernel-shape choice for (n_atoms, nq, precision): the q-block length K of
+ * the recurrence and the atom-chunk length of a tile, as picked by the
+ * context's autotuner cache (pd_autotune fills it by timing candidates on the
+ * device). Host-only for pd_get_tuning. */
+int pd_get_tuning(pd_ctx *ctx, uint64_t n_atoms, uint64_t nq, uint32_t precision,
+                  uint32_t *q_block, uint32_t *j_chunk);
+int pd_set_tuning(pd_ctx *ctx, uint64_t n_atoms, uint64_t nq, uint32_t precision,
+                  uint32_t q_block, uint32_t j_chunk);
+int pd_autotune(pd_ctx *ctx, uint64_t n_atoms, uint64_t nq, uint32_t precision);
+
+/* Host-only planning report for a request (no device work): number of atom
+ * classes (species × hydration weight), padded atom count, tiles launched and
+ * the unordered pairs those tiles cover in total, which must equal
+ * N(N-1)/2. ctx may be NULL (default tuning). */
+int pd_plan_inspect(pd_ctx *ctx, const pd_request *req, uint64_t *n_classes,
+                    uint64_t *n_padded, uint64_t *n_tiles, uint64_t *pairs_covered);
+
+/* Measured FP32 issue peak of the device: FFMA throughput of a register-only
+ * microbenchmark, in TFLOP/s at the clock the device runs during the call. */
+int pd_measure_fp32_peak(pd_ctx *ctx, double *tflops_ffma, double *tflops_ffma2);
+
+/* Number of kernel launches the context has issued since creation. */
+uint64_t pd_launch_count(pd_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PRIPPS_DEBYE_H */

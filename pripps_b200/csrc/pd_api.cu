@@ -1,0 +1,1224 @@
+// C ABI of the Debye backend: context, device arena, plan upload and
+// execution, blocking solve, the continuous-batching request loop, the
+// autotuner and the FP32 peak probe. Declarations and contracts are in
+// include/pripps_debye.h.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <condition_variable>
+#include <cstdio>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <random>
+#include <string>
+#include <thread>
+#include <tuple>
+#include <unordered_map>
+#include <vector>
+
+#include "pd_common.h"
+#include "pd_kernels.h"
+#include "pd_plan.h"
+#include "pripps_debye.h"
+
+using pd::Plan;
+using pd::Tuning;
+
+namespace {
+
+std::mutex g_err_mu;
+std::string g_err;  // context-free failures (pd_ctx_create)
+
+double now_s() {
+    using clk = std::chrono::steady_clock;
+    static const clk::time_point t0 = clk::now();
+    return std::chrono::duration<double>(clk::now() - t0).count();
+}
+
+inline uint64_t align_up(uint64_t v, uint64_t a) { return (v + a - 1) / a * a; }
+
+// Offsets of every array of one request inside its single device chunk. The
+// first `upload_bytes` bytes mirror a host staging image uploaded with one
+// copy; the rest is device-only scratch.
+struct Layout {
+    uint64_t qv, ffA, ffC, ffW, hw, fw, cls, pairs, perm, gvalid, jobs, lptr, lidx, req, njobs,
+        xyz;
+    uint64_t upload_bytes;
+    uint64_t hres;         // host-only: pinned landing area of the [6][nq] result
+    uint64_t stage_bytes;  // pinned image size (upload + result area)
+    uint64_t centroid, atoms, slots, pairsum, terms, out, counter;
+    uint64_t total;
+};
+
+Layout make_layout(const Plan &P, bool host_xyz) {
+    Layout L{};
+    uint64_t o = 0;
+    auto take = [&](uint64_t bytes) {
+        const uint64_t at = o;
+        o = align_up(o + std::max<uint64_t>(bytes, 1), 256);
+        return at;
+    };
+    const uint64_t nq = P.nq, S = P.n_species;
+    L.qv = take(nq * 8);
+    L.ffA = take(S * nq * 8);
+    L.ffC = take(P.has_exc ? S * nq * 8 : 0);
+    L.ffW = take(P.has_hyd ? nq * 8 : 0);
+    L.hw = take(P.has_hyd ? static_cast<uint64_t>(P.n_atoms) * 8 : 0);
+    L.fw = take(static_cast<uint64_t>(P.n_frames) * 8);
+    L.cls = take(P.cls.size() * sizeof(PdClassDev));
+    L.pairs = take(P.pairs.size() * sizeof(PdPairDev));
+    L.perm = take(P.perm.size() * 4);
+    L.gvalid = take(P.gvalid.size() * 4);
+    L.jobs = take(P.jobs.size() * sizeof(PdJob));
+    L.lptr = take(P.lptr.size() * 8);
+    L.lidx = take(P.lidx.size() * 8);
+    L.req = take(sizeof(PdReqDev));
+    L.njobs = take(sizeof(int));
+    L.xyz = take(host_xyz ? static_cast<uint64_t>(P.n_atoms) * 3 * P.n_frames * 8 : 0);
+    L.upload_bytes = o;
+    L.hres = o;
+    L.stage_bytes = align_up(o + 6 * nq * 8, 256);
+    L.centroid = take(static_cast<uint64_t>(P.n_frames) * 3 * 8);
+    L.atoms = take(static_cast<uint64_t>(P.n_pad) * P.n_frames *
+                   (P.precision == PD_FP64 ? sizeof(double4) : sizeof(float4)));
+    L.slots = take(static_cast<uint64_t>(P.slots_per_frame) * P.n_frames * P.nv * P.tun.K * 8);
+    L.pairsum = take(static_cast<uint64_t>(P.n_frames) * P.nv * P.n_pairs * nq * 8);
+    L.terms = take(static_cast<uint64_t>(P.n_frames) * 6 * nq * 8);
+    L.out = take(6 * nq * 8);
+    L.counter = take(sizeof(int) * 4);
+    L.total = o;
+    return L;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- context
+struct PdTicket;
+
+struct pd_ctx {
+    int device = 0;
+    int sm_count = 0;
+    uint64_t budget = 0;
+    std::atomic<uint64_t> in_use{0};
+    std::atomic<uint64_t> launches{0};
+    cudaStream_t stream = nullptr;  // blocking solves and the request loop
+    cudaMemPool_t pool = nullptr;
+
+    std::mutex mu;  // tuning table, per-thread errors
+    std::map<std::tuple<int, int, int>, Tuning> tuning;
+    std::unordered_map<std::thread::id, std::string> errors;
+    std::mutex solve_mu;  // serialises blocking solves on `stream`
+
+    // request loop
+    std::mutex qmu;
+    std::condition_variable qcv;
+    std::condition_variable done_cv;
+    std::deque<uint64_t> pending;
+    std::map<uint64_t, std::shared_ptr<PdTicket>> tickets;
+    uint64_t next_ticket = 1;
+    bool stop = false;
+    std::thread worker;
+    bool worker_started = false;
+
+    void set_error(const std::string &m) {
+        std::lock_guard<std::mutex> g(mu);
+        errors[std::this_thread::get_id()] = m;
+    }
+};
+
+namespace {
+
+int cuda_fail(pd_ctx *ctx, cudaError_t e, const char *what) {
+    std::string m = std::string(what) + ": " + cudaGetErrorString(e);
+    if (ctx) ctx->set_error(m);
+    return PD_EDEVICE;
+}
+
+#define PD_CUDA(ctx, call)                                  \
+    do {                                                    \
+        cudaError_t e__ = (call);                           \
+        if (e__ != cudaSuccess) return cuda_fail(ctx, e__, #call); \
+    } while (0)
+
+// One planned request resident on the device.
+struct DevPlan {
+    Plan P;
+    Layout L{};
+    char *base = nullptr;   // device chunk
+    char *stage = nullptr;  // pinned host image of the uploaded part
+    uint64_t charged = 0;
+    bool host_xyz = false;
+    const double *xyz_dev = nullptr;  // coordinates used by pack
+    template <class T>
+    T *dptr(uint64_t off) const {
+        return reinterpret_cast<T *>(base + off);
+    }
+    template <class T>
+    T *hptr(uint64_t off) const {
+        return reinterpret_cast<T *>(stage + off);
+    }
+};
+
+Tuning tuning_for(pd_ctx *ctx, int64_t n, int64_t nq, int precision) {
+    const int nb = static_cast<int>(std::floor(std::log2(static_cast<double>(std::max<int64_t>(n, 1)))));
+    const int qb = static_cast<int>(std::floor(std::log2(static_cast<double>(std::max<int64_t>(nq, 1)))));
+    if (ctx) {
+        std::lock_guard<std::mutex> g(ctx->mu);
+        auto it = ctx->tuning.find(std::make_tuple(precision, nb, qb));
+        if (it != ctx->tuning.end()) {
+            Tuning t = it->second;
+            if (precision != PD_FP64 && nq <= 32) t.K = 32;
+            return t;
+        }
+    }
+    return pd::default_tuning(n, nq, precision);
+}
+
+void free_devplan(pd_ctx *ctx, DevPlan &dp, cudaStream_t st) {
+    if (dp.base) cudaFreeAsync(dp.base, st);
+    if (dp.stage) cudaFreeHost(dp.stage);
+    dp.base = nullptr;
+    dp.stage = nullptr;
+    if (dp.charged) ctx->in_use.fetch_sub(dp.charged);
+    dp.charged = 0;
+}
+
+// Fill the pinned staging image (tables, layout, tiles, lists, descriptor).
+int stage_plan(pd_ctx *ctx, DevPlan &dp, const pd_request *req) {
+    const Plan &P = dp.P;
+    const Layout &L = dp.L;
+    std::memcpy(dp.hptr<double>(L.qv), P.qv.data(), P.qv.size() * 8);
+    const size_t tab = static_cast<size_t>(P.n_species) * P.nq;
+    std::memcpy(dp.hptr<double>(L.ffA), req->ff_atoms, tab * 8);
+    if (P.has_exc) std::memcpy(dp.hptr<double>(L.ffC), req->ff_excluded, tab * 8);
+    if (P.has_hyd) {
+        std::memcpy(dp.hptr<double>(L.ffW), req->ff_water, static_cast<size_t>(P.nq) * 8);
+        std::memcpy(dp.hptr<double>(L.hw), req->hyd_weights, static_cast<size_t>(P.n_atoms) * 8);
+    }
+    double *fw = dp.hptr<double>(L.fw);
+    for (int f = 0; f < P.n_frames; ++f) fw[f] = req->frame_weights ? req->frame_weights[f] : 1.0;
+    std::memcpy(dp.hptr<char>(L.cls), P.cls.data(), P.cls.size() * sizeof(PdClassDev));
+    std::memcpy(dp.hptr<char>(L.pairs), P.pairs.data(), P.pairs.size() * sizeof(PdPairDev));
+    std::memcpy(dp.hptr<char>(L.perm), P.perm.data(), P.perm.size() * 4);
+    std::memcpy(dp.hptr<char>(L.gvalid), P.gvalid.data(), P.gvalid.size() * 4);
+    std::memcpy(dp.hptr<char>(L.jobs), P.jobs.data(), P.jobs.size() * sizeof(PdJob));
+    std::memcpy(dp.hptr<char>(L.lptr), P.lptr.data(), P.lptr.size() * 8);
+    std::memcpy(dp.hptr<char>(L.lidx), P.lidx.data(), P.lidx.size() * 8);
+    PdReqDev rd{};
+    if (P.precision == PD_FP64)
+        rd.atoms64 = dp.dptr<double4>(L.atoms);
+    else
+        rd.atoms32 = dp.dptr<float4>(L.atoms);
+    rd.gvalid = dp.dptr<int32_t>(L.gvalid);
+    rd.qv = dp.dptr<double>(L.qv);
+    rd.slots = dp.dptr<double>(L.slots);
+    rd.qmin = P.qmin;
+    rd.dq = P.dq;
+    rd.n_pad = P.n_pad;
+    rd.nq = P.nq;
+    rd.K = P.tun.K;
+    rd.mode = P.mode;
+    std::memcpy(dp.hptr<char>(L.req), &rd, sizeof(rd));
+    const int nj = static_cast<int>(P.jobs.size());
+    std::memcpy(dp.hptr<char>(L.njobs), &nj, sizeof(int));
+    if (dp.host_xyz)
+        std::memcpy(dp.hptr<double>(L.xyz), req->xyz,
+                    static_cast<size_t>(P.n_atoms) * 3 * P.n_frames * 8);
+    (void)ctx;
+    return PD_OK;
+}
+
+constexpr int kBudgetWait = -100;  // internal: does not fit the budget right now
+
+// Host planning only: tiles, lists and the device layout.
+int plan_host(pd_ctx *ctx, const pd_request *req, const uint32_t *species, const double *weights,
+              bool host_xyz, DevPlan &dp) {
+    std::string msg;
+    Tuning tun = tuning_for(ctx, static_cast<int64_t>(req->n_atoms),
+                            static_cast<int64_t>(req->nq), static_cast<int>(req->precision));
+    int rc = pd::build_plan(req, species, weights, tun, dp.P, msg);
+    if (rc != PD_OK) {
+        ctx->set_error(msg);
+        return rc;
+    }
+    dp.host_xyz = host_xyz;
+    dp.L = make_layout(dp.P, host_xyz);
+    if (dp.L.total > ctx->budget) {
+        ctx->set_error("request needs " + std::to_string(dp.L.total) +
+                       " device bytes, the budget is " + std::to_string(ctx->budget));
+        return PD_EBUDGET;
+    }
+    return PD_OK;
+}
+
+// Charge the budget, allocate the device chunk and the pinned image, stage and
+// upload. With `wait` a full budget returns kBudgetWait (retry after frees);
+// without it a full budget is PD_EBUDGET.
+int plan_device(pd_ctx *ctx, const pd_request *req, DevPlan &dp, cudaStream_t st, bool wait) {
+    const uint64_t need = dp.L.total;
+    uint64_t cur = ctx->in_use.load();
+    for (;;) {
+        if (cur + need > ctx->budget) {
+            if (wait) return kBudgetWait;
+            ctx->set_error("device memory budget exhausted");
+            return PD_EBUDGET;
+        }
+        if (ctx->in_use.compare_exchange_weak(cur, cur + need)) break;
+    }
+    dp.charged = need;
+    cudaError_t e = cudaMallocFromPoolAsync(reinterpret_cast<void **>(&dp.base), need, ctx->pool, st);
+    if (e != cudaSuccess) {
+        free_devplan(ctx, dp, st);
+        ctx->set_error(std::string("device allocation failed: ") + cudaGetErrorString(e));
+        return PD_ENOMEM;
+    }
+    e = cudaHostAlloc(reinterpret_cast<void **>(&dp.stage), dp.L.stage_bytes, cudaHostAllocDefault);
+    if (e != cudaSuccess) {
+        free_devplan(ctx, dp, st);
+        ctx->set_error(std::string("pinned allocation failed: ") + cudaGetErrorString(e));
+        return PD_ENOMEM;
+    }
+    stage_plan(ctx, dp, req);
+    e = cudaMemcpyAsync(dp.base, dp.stage, dp.L.upload_bytes, cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) {
+        free_devplan(ctx, dp, st);
+        return cuda_fail(ctx, e, "plan upload");
+    }
+    if (dp.host_xyz) dp.xyz_dev = dp.dptr<double>(dp.L.xyz);
+    return PD_OK;
+}
+
+int create_devplan(pd_ctx *ctx, const pd_request *req, const uint32_t *species,
+                   const double *weights, bool host_xyz, DevPlan &dp, cudaStream_t st) {
+    int rc = plan_host(ctx, req, species, weights, host_xyz, dp);
+    if (rc) return rc;
+    return plan_device(ctx, req, dp, st, false);
+}
+
+// Everything after the pair kernel: slot reduction, six-profile combine and
+// the frame mean; leaves the [6][nq] result at L.out (or out_dev).
+int finish_devplan(pd_ctx *ctx, DevPlan &dp, double *out_dev, cudaStream_t st) {
+    const Plan &P = dp.P;
+    const Layout &L = dp.L;
+    PD_CUDA(ctx, pd::launch_reduce(dp.dptr<double>(L.slots), dp.dptr<int64_t>(L.lptr),
+                                   dp.dptr<int64_t>(L.lidx), dp.dptr<PdPairDev>(L.pairs),
+                                   dp.dptr<double>(L.qv), P.n_pairs, P.nq, P.tun.K, P.nv,
+                                   P.n_frames, P.slots_per_frame, dp.dptr<double>(L.pairsum), st));
+    PD_CUDA(ctx, pd::launch_combine(dp.dptr<double>(L.pairsum), dp.dptr<PdClassDev>(L.cls),
+                                    dp.dptr<PdPairDev>(L.pairs), P.n_cls, P.n_pairs, P.nq, P.nv,
+                                    P.n_frames, dp.dptr<double>(L.ffA),
+                                    P.has_exc ? dp.dptr<double>(L.ffC) : nullptr,
+                                    P.has_hyd ? dp.dptr<double>(L.ffW) : nullptr,
+                                    dp.dptr<double>(L.terms), st));
+    ctx->launches += 2;
+    double *dst = out_dev ? out_dev : dp.dptr<double>(L.out);
+    if (P.n_frames > 1) {
+        PD_CUDA(ctx, pd::launch_frame_mean(dp.dptr<double>(L.terms), dp.dptr<double>(L.fw),
+                                           P.n_frames, P.nq, dst, st));
+        ctx->launches += 1;
+    } else {
+        PD_CUDA(ctx, cudaMemcpyAsync(dst, dp.dptr<double>(L.terms),
+                                     static_cast<size_t>(6) * P.nq * 8,
+                                     cudaMemcpyDeviceToDevice, st));
+    }
+    return PD_OK;
+}
+
+// centroid + pack of the coordinates into the padded class layout.
+int pack_devplan(pd_ctx *ctx, DevPlan &dp, cudaStream_t st) {
+    const Plan &P = dp.P;
+    const Layout &L = dp.L;
+    PD_CUDA(ctx, pd::launch_centroid(dp.xyz_dev, P.n_atoms, P.n_frames, dp.dptr<double>(L.centroid), st));
+    PD_CUDA(ctx, pd::launch_pack(dp.xyz_dev, P.has_hyd ? dp.dptr<double>(L.hw) : nullptr,
+                                 dp.dptr<int32_t>(L.perm), dp.dptr<double>(L.centroid), P.n_atoms,
+                                 P.n_pad, P.n_frames,
+                                 P.precision == PD_FP64 ? nullptr : dp.dptr<float4>(L.atoms),
+                                 P.precision == PD_FP64 ? dp.dptr<double4>(L.atoms) : nullptr, st));
+    ctx->launches += 2;
+    return PD_OK;
+}
+
+int persistent_grid(pd_ctx *ctx, const Plan &P, int64_t n_jobs) {
+    const int per_sm = std::max(1, pd::pairs_blocks_per_sm(P.precision, P.tun.K, P.mode));
+    const int64_t g = std::min<int64_t>(n_jobs, static_cast<int64_t>(ctx->sm_count) * per_sm);
+    return static_cast<int>(std::max<int64_t>(g, 1));
+}
+
+// The whole device pipeline of one plan on stream st; ev (optional) brackets
+// the pair kernel.
+int run_devplan(pd_ctx *ctx, DevPlan &dp, double *out_dev, cudaStream_t st,
+                std::pair<cudaEvent_t, cudaEvent_t> *ev = nullptr) {
+    const Plan &P = dp.P;
+    const Layout &L = dp.L;
+    int rc = pack_devplan(ctx, dp, st);
+    if (rc) return rc;
+    if (ev) cudaEventRecord(ev->first, st);
+    if (!P.jobs.empty()) {
+        PD_CUDA(ctx, cudaMemsetAsync(dp.dptr<int>(L.counter), 0, sizeof(int), st));
+        PD_CUDA(ctx, pd::launch_pairs(P.precision, P.tun.K, P.mode, dp.dptr<PdJob>(L.jobs),
+                                      dp.dptr<int>(L.njobs), dp.dptr<PdReqDev>(L.req),
+                                      dp.dptr<int>(L.counter),
+                                      persistent_grid(ctx, P, static_cast<int64_t>(P.jobs.size())),
+                                      st));
+        ctx->launches += 1;
+    }
+    if (ev) cudaEventRecord(ev->second, st);
+    return finish_devplan(ctx, dp, out_dev, st);
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- plan API
+struct pd_plan {
+    DevPlan dp;
+    bool profiling = false;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pair_events;  // one per execution
+};
+
+// ---------------------------------------------------------------- request loop
+struct PdTicket {
+    uint64_t id = 0;
+    pd_request req{};                 // pointers below own the copies
+    std::vector<double> xyz, ffA, ffC, hw, ffW, fw;
+    std::vector<uint32_t> species;
+    DevPlan dp;
+    int status = 1;                   // 1 pending/running, 0 done, < 0 error
+    bool planned = false;
+    bool admitted = false;
+    bool canceled = false;
+    bool taken = false;               // result copied out by pd_wait
+    size_t next_job = 0;              // first tile not yet issued
+    bool finish_issued = false;
+    cudaEvent_t done_ev = nullptr;
+    std::vector<double> result;
+    std::string err;
+    double t_submit = 0, t_admit = 0, t_done = 0;
+};
+
+namespace {
+
+// Step buffers of the request loop: tiles of several requests plus the
+// descriptor array they index, uploaded from pinned memory and run by a
+// captured graph (upload, counter reset, persistent pair kernel).
+struct StepBuf {
+    PdJob *h_jobs = nullptr, *d_jobs = nullptr;
+    PdReqDev *h_reqs = nullptr, *d_reqs = nullptr;
+    int *h_n = nullptr, *d_n = nullptr;
+    int *d_counter = nullptr;
+    size_t cap_jobs = 0, cap_reqs = 0;
+    cudaEvent_t ev = nullptr;
+    bool busy = false;
+    std::map<std::tuple<int, int, int>, cudaGraphExec_t> graphs;  // (precision, K, mode)
+};
+
+constexpr size_t STEP_MAX_JOBS = 1 << 14;
+constexpr size_t STEP_MAX_REQS = 1024;
+constexpr double STEP_PAIRQ = 4.0e10;  // ≈ 5 ms of FP32 work per step
+
+void ticket_fail(pd_ctx *ctx, const std::shared_ptr<PdTicket> &t, int code, const std::string &m,
+                 cudaStream_t st) {
+    t->status = code;
+    t->err = m;
+    t->t_done = now_s();
+    if (t->dp.base || t->dp.stage) free_devplan(ctx, t->dp, st);
+}
+
+int step_graph(pd_ctx *ctx, StepBuf &sb, int precision, int K, int mode, cudaStream_t st,
+               cudaGraphExec_t *out) {
+    auto key = std::make_tuple(precision, K, mode);
+    auto it = sb.graphs.find(key);
+    if (it != sb.graphs.end()) {
+        *out = it->second;
+        return PD_OK;
+    }
+    Plan dummy;
+    dummy.precision = precision;
+    dummy.tun.K = K;
+    dummy.mode = mode;
+    const int grid = persistent_grid(ctx, dummy, 1 << 30);
+    cudaGraph_t g = nullptr;
+    PD_CUDA(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    cudaMemcpyAsync(sb.d_n, sb.h_n, sizeof(int), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(sb.d_reqs, sb.h_reqs, sb.cap_reqs * sizeof(PdReqDev), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(sb.d_jobs, sb.h_jobs, sb.cap_jobs * sizeof(PdJob), cudaMemcpyHostToDevice, st);
+    cudaMemsetAsync(sb.d_counter, 0, sizeof(int), st);
+    pd::launch_pairs(precision, K, mode, sb.d_jobs, sb.d_n, sb.d_reqs, sb.d_counter, grid, st);
+    PD_CUDA(ctx, cudaStreamEndCapture(st, &g));
+    cudaGraphExec_t ge = nullptr;
+    cudaError_t e = cudaGraphInstantiate(&ge, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaGraphInstantiate");
+    sb.graphs[key] = ge;
+    *out = ge;
+    return PD_OK;
+}
+
+void worker_main(pd_ctx *ctx) {
+    cudaSetDevice(ctx->device);
+    cudaStream_t st = nullptr;
+    cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    StepBuf sbuf[2];
+    bool init_ok = true;
+    for (auto &sb : sbuf) {
+        sb.cap_jobs = STEP_MAX_JOBS;
+        sb.cap_reqs = STEP_MAX_REQS;
+        init_ok &= cudaHostAlloc(reinterpret_cast<void **>(&sb.h_jobs), sb.cap_jobs * sizeof(PdJob), 0) == cudaSuccess;
+        init_ok &= cudaHostAlloc(reinterpret_cast<void **>(&sb.h_reqs), sb.cap_reqs * sizeof(PdReqDev), 0) == cudaSuccess;
+        init_ok &= cudaHostAlloc(reinterpret_cast<void **>(&sb.h_n), sizeof(int), 0) == cudaSuccess;
+        init_ok &= cudaMalloc(reinterpret_cast<void **>(&sb.d_jobs), sb.cap_jobs * sizeof(PdJob)) == cudaSuccess;
+        init_ok &= cudaMalloc(reinterpret_cast<void **>(&sb.d_reqs), sb.cap_reqs * sizeof(PdReqDev)) == cudaSuccess;
+        init_ok &= cudaMalloc(reinterpret_cast<void **>(&sb.d_n), sizeof(int)) == cudaSuccess;
+        init_ok &= cudaMalloc(reinterpret_cast<void **>(&sb.d_counter), sizeof(int)) == cudaSuccess;
+        init_ok &= cudaEventCreateWithFlags(&sb.ev, cudaEventDisableTiming) == cudaSuccess;
+    }
+    std::vector<std::shared_ptr<PdTicket>> active;  // admitted, in admission order
+    int cur = 0;
+    for (;;) {
+        std::vector<std::shared_ptr<PdTicket>> admit_try;
+        {
+            std::unique_lock<std::mutex> lk(ctx->qmu);
+            if (active.empty() && ctx->pending.empty() && !ctx->stop)
+                ctx->qcv.wait_for(lk, std::chrono::milliseconds(50));
+            if (ctx->stop) break;
+            // drop cancelled pending tickets
+            for (auto it = ctx->pending.begin(); it != ctx->pending.end();) {
+                auto t = ctx->tickets[*it];
+                if (t->canceled) {
+                    t->status = PD_ECANCELED;
+                    t->t_done = now_s();
+                    it = ctx->pending.erase(it);
+                    ctx->done_cv.notify_all();
+                } else {
+                    ++it;
+                }
+            }
+            for (uint64_t id : ctx->pending) admit_try.push_back(ctx->tickets[id]);
+        }
+        if (!init_ok) {
+            std::lock_guard<std::mutex> lk(ctx->qmu);
+            for (auto &t : admit_try) {
+                t->status = PD_ENOMEM;
+                t->err = "request loop could not allocate its step buffers";
+                ctx->pending.erase(std::find(ctx->pending.begin(), ctx->pending.end(), t->id));
+            }
+            ctx->done_cv.notify_all();
+            continue;
+        }
+        // ---- admission in FIFO order while the budget allows
+        for (auto &t : admit_try) {
+            int rc = PD_OK;
+            if (!t->planned) {
+                rc = plan_host(ctx, &t->req, t->req.species, t->req.hyd_weights, true, t->dp);
+                t->planned = (rc == PD_OK);
+            }
+            if (rc == PD_OK) rc = plan_device(ctx, &t->req, t->dp, st, /*wait=*/true);
+            if (rc == kBudgetWait) break;  // keep FIFO order; retry after frees
+            std::lock_guard<std::mutex> lk(ctx->qmu);
+            ctx->pending.pop_front();
+            if (rc != PD_OK) {
+                std::string m;
+                {
+                    std::lock_guard<std::mutex> g(ctx->mu);
+                    m = ctx->errors[std::this_thread::get_id()];
+                }
+                ticket_fail(ctx, t, rc, m, st);
+                ctx->done_cv.notify_all();
+                continue;
+            }
+            if (pack_devplan(ctx, t->dp, st) != PD_OK) {
+                ticket_fail(ctx, t, PD_EDEVICE, "pack failed", st);
+                ctx->done_cv.notify_all();
+                continue;
+            }
+            // the device and the pinned image hold the inputs now
+            t->xyz = {};
+            t->ffA = {};
+            t->ffC = {};
+            t->hw = {};
+            t->ffW = {};
+            t->fw = {};
+            t->species = {};
+            t->admitted = true;
+            t->t_admit = now_s();
+            active.push_back(t);
+        }
+        if (active.empty()) continue;
+        // ---- one step: tiles of the active requests, round-robin in chunks
+        StepBuf &sb = sbuf[cur];
+        if (sb.busy) {
+            cudaEventSynchronize(sb.ev);
+            sb.busy = false;
+        }
+        // Group by kernel variant; a step runs one variant (the oldest
+        // request's) so that one captured graph covers it.
+        std::shared_ptr<PdTicket> head;
+        for (auto &t : active)
+            if (!t->canceled && t->next_job < t->dp.P.jobs.size()) {
+                head = t;
+                break;
+            }
+        std::vector<std::shared_ptr<PdTicket>> finished_now;
+        if (head) {
+            const int prec = head->dp.P.precision, K = head->dp.P.tun.K, mode = head->dp.P.mode;
+            std::vector<std::shared_ptr<PdTicket>> members;
+            for (auto &t : active)
+                if (!t->canceled && t->next_job < t->dp.P.jobs.size() &&
+                    t->dp.P.precision == prec && t->dp.P.tun.K == K && t->dp.P.mode == mode &&
+                    members.size() < STEP_MAX_REQS)
+                    members.push_back(t);
+            size_t nj = 0;
+            double work = 0;
+            // Round-robin: every member contributes tiles in turn so that a
+            // newly admitted small request is not starved by a large one.
+            bool progress = true;
+            while (progress && nj < STEP_MAX_JOBS && work < STEP_PAIRQ) {
+                progress = false;
+                for (size_t m = 0; m < members.size(); ++m) {
+                    auto &t = members[m];
+                    const auto &jobs = t->dp.P.jobs;
+                    size_t take = 0;
+                    while (t->next_job < jobs.size() && nj < STEP_MAX_JOBS && take < 64) {
+                        PdJob jb = jobs[t->next_job++];
+                        jb.req = static_cast<int32_t>(m);
+                        sb.h_jobs[nj++] = jb;
+                        work += static_cast<double>(PD_IBLOCK) * (jb.j1 - jb.j0) * K;
+                        ++take;
+                        progress = true;
+                    }
+                    if (work >= STEP_PAIRQ || nj >= STEP_MAX_JOBS) break;
+                }
+            }
+            for (size_t m = 0; m < members.size(); ++m) {
+                std::memcpy(&sb.h_reqs[m], members[m]->dp.hptr<char>(members[m]->dp.L.req),
+                            sizeof(PdReqDev));
+            }
+            *sb.h_n = static_cast<int>(nj);
+            cudaGraphExec_t ge = nullptr;
+            int rc = step_graph(ctx, sb, prec, K, mode, st, &ge);
+            if (rc == PD_OK && cudaGraphLaunch(ge, st) == cudaSuccess) {
+                ctx->launches += 1;
+            } else {
+                std::lock_guard<std::mutex> lk(ctx->qmu);
+                for (auto &t : members) ticket_fail(ctx, t, PD_EDEVICE, "step launch failed", st);
+                ctx->done_cv.notify_all();
+            }
+            for (auto &t : members)
+                if (t->status == 1 && t->next_job >= t->dp.P.jobs.size()) finished_now.push_back(t);
+        }
+        // requests with no tiles at all (N = 1) finish right away
+        for (auto &t : active)
+            if (t->status == 1 && !t->finish_issued && t->dp.P.jobs.empty())
+                finished_now.push_back(t);
+        for (auto &t : finished_now) {
+            if (finish_devplan(ctx, t->dp, nullptr, st) != PD_OK) {
+                std::lock_guard<std::mutex> lk(ctx->qmu);
+                ticket_fail(ctx, t, PD_EDEVICE, "reduction launch failed", st);
+                ctx->done_cv.notify_all();
+                continue;
+            }
+            cudaMemcpyAsync(t->dp.hptr<double>(t->dp.L.hres), t->dp.dptr<double>(t->dp.L.out),
+                            static_cast<size_t>(6) * t->dp.P.nq * 8, cudaMemcpyDeviceToHost, st);
+            cudaEventCreateWithFlags(&t->done_ev, cudaEventDisableTiming);
+            cudaEventRecord(t->done_ev, st);
+            t->finish_issued = true;
+        }
+        cudaEventRecord(sb.ev, st);
+        sb.busy = true;
+        cur ^= 1;
+        // ---- retire finished and cancelled requests
+        for (auto it = active.begin(); it != active.end();) {
+            auto &t = *it;
+            bool remove = false;
+            if (t->status < 0) {
+                remove = true;
+            } else if (t->finish_issued && cudaEventQuery(t->done_ev) == cudaSuccess) {
+                cudaEventDestroy(t->done_ev);
+                t->done_ev = nullptr;
+                const double *res = t->dp.hptr<double>(t->dp.L.hres);
+                t->result.assign(res, res + static_cast<size_t>(6) * t->dp.P.nq);
+                free_devplan(ctx, t->dp, st);
+                std::lock_guard<std::mutex> lk(ctx->qmu);
+                t->status = 0;
+                t->t_done = now_s();
+                ctx->done_cv.notify_all();
+                remove = true;
+            } else if (t->canceled && !t->finish_issued) {
+                // tiles already issued may still run: wait for the stream
+                cudaStreamSynchronize(st);
+                free_devplan(ctx, t->dp, st);
+                std::lock_guard<std::mutex> lk(ctx->qmu);
+                t->status = PD_ECANCELED;
+                t->t_done = now_s();
+                ctx->done_cv.notify_all();
+                remove = true;
+            }
+            it = remove ? active.erase(it) : it + 1;
+        }
+        // When nothing new can be issued, wait for the GPU instead of spinning.
+        bool any_issuable = false;
+        for (auto &t : active)
+            if (!t->canceled && t->next_job < t->dp.P.jobs.size()) any_issuable = true;
+        if (!any_issuable && !active.empty()) {
+            bool pending_new;
+            {
+                std::lock_guard<std::mutex> lk(ctx->qmu);
+                pending_new = !ctx->pending.empty();
+            }
+            if (!pending_new) {
+                for (auto &t : active)
+                    if (t->done_ev) {
+                        cudaEventSynchronize(t->done_ev);
+                        break;
+                    }
+            }
+        }
+    }
+    cudaStreamSynchronize(st);
+    for (auto &t : active) free_devplan(ctx, t->dp, st);
+    for (auto &sb : sbuf) {
+        for (auto &kv : sb.graphs) cudaGraphExecDestroy(kv.second);
+        cudaFreeHost(sb.h_jobs);
+        cudaFreeHost(sb.h_reqs);
+        cudaFreeHost(sb.h_n);
+        cudaFree(sb.d_jobs);
+        cudaFree(sb.d_reqs);
+        cudaFree(sb.d_n);
+        cudaFree(sb.d_counter);
+        if (sb.ev) cudaEventDestroy(sb.ev);
+    }
+    cudaStreamDestroy(st);
+}
+
+}  // namespace
+
+// ====================================================================== ABI
+extern "C" {
+
+int pd_ctx_create(int device, uint64_t mem_budget_bytes, pd_ctx **out) {
+    if (!out) return PD_EINVAL;
+    *out = nullptr;
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || device < 0 || device >= count) {
+        std::lock_guard<std::mutex> g(g_err_mu);
+        g_err = std::string("no CUDA device ") + std::to_string(device) +
+                (e != cudaSuccess ? std::string(": ") + cudaGetErrorString(e) : std::string());
+        return PD_ENODEV;
+    }
+    cudaDeviceProp prop{};
+    cudaGetDeviceProperties(&prop, device);
+    if (prop.major < 10) {
+        std::lock_guard<std::mutex> g(g_err_mu);
+        g_err = "device " + std::to_string(device) + " is sm_" + std::to_string(prop.major) +
+                std::to_string(prop.minor) + "; this library is built for sm_100a";
+        return PD_ENODEV;
+    }
+    auto *ctx = new pd_ctx();
+    ctx->device = device;
+    ctx->sm_count = prop.multiProcessorCount;
+    cudaSetDevice(device);
+    size_t free_b = 0, total_b = 0;
+    cudaMemGetInfo(&free_b, &total_b);
+    ctx->budget = mem_budget_bytes ? mem_budget_bytes : static_cast<uint64_t>(free_b * 0.9);
+    e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) {
+        cudaMemPoolProps pp{};
+        pp.allocType = cudaMemAllocationTypePinned;
+        pp.handleTypes = cudaMemHandleTypeNone;
+        pp.location.type = cudaMemLocationTypeDevice;
+        pp.location.id = device;
+        e = cudaMemPoolCreate(&ctx->pool, &pp);
+        if (e == cudaSuccess) {
+            uint64_t thr = UINT64_MAX;
+            cudaMemPoolSetAttribute(ctx->pool, cudaMemPoolAttrReleaseThreshold, &thr);
+        }
+    }
+    if (e != cudaSuccess) {
+        std::lock_guard<std::mutex> g(g_err_mu);
+        g_err = std::string("context setup failed: ") + cudaGetErrorString(e);
+        if (ctx->stream) cudaStreamDestroy(ctx->stream);
+        delete ctx;
+        return PD_EDEVICE;
+    }
+    *out = ctx;
+    return PD_OK;
+}
+
+void pd_ctx_destroy(pd_ctx *ctx) {
+    if (!ctx) return;
+    {
+        std::lock_guard<std::mutex> lk(ctx->qmu);
+        ctx->stop = true;
+        for (auto &kv : ctx->tickets)
+            if (kv.second->status == 1) kv.second->canceled = true;
+    }
+    ctx->qcv.notify_all();
+    if (ctx->worker_started) ctx->worker.join();
+    {
+        std::lock_guard<std::mutex> lk(ctx->qmu);
+        for (auto &kv : ctx->tickets)
+            if (kv.second->status == 1) kv.second->status = PD_ECANCELED;
+        ctx->done_cv.notify_all();
+    }
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    cudaStreamDestroy(ctx->stream);
+    if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
+    delete ctx;
+}
+
+const char *pd_last_error(pd_ctx *ctx) {
+    static thread_local std::string copy;
+    if (!ctx) {
+        std::lock_guard<std::mutex> g(g_err_mu);
+        copy = g_err;
+        return copy.c_str();
+    }
+    std::lock_guard<std::mutex> g(ctx->mu);
+    auto it = ctx->errors.find(std::this_thread::get_id());
+    copy = it == ctx->errors.end() ? std::string() : it->second;
+    return copy.c_str();
+}
+
+int pd_solve(pd_ctx *ctx, const pd_request *req, double *out_terms) {
+    if (!ctx || !out_terms) return PD_EINVAL;
+    std::string msg;
+    int rc = pd::validate_request(req, false, msg);
+    if (rc) {
+        ctx->set_error(msg);
+        return rc;
+    }
+    std::lock_guard<std::mutex> g(ctx->solve_mu);
+    cudaSetDevice(ctx->device);
+    DevPlan dp;
+    rc = create_devplan(ctx, req, req->species, req->hyd_weights, true, dp, ctx->stream);
+    if (rc) return rc;
+    rc = run_devplan(ctx, dp, nullptr, ctx->stream);
+    if (rc == PD_OK) {
+        cudaError_t e = cudaMemcpyAsync(out_terms, dp.dptr<double>(dp.L.out),
+                                        static_cast<size_t>(6) * dp.P.nq * 8,
+                                        cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) rc = cuda_fail(ctx, e, "pd_solve");
+    }
+    free_devplan(ctx, dp, ctx->stream);
+    cudaStreamSynchronize(ctx->stream);
+    return rc;
+}
+
+int pd_plan_create(pd_ctx *ctx, const pd_request *req, pd_plan **out) {
+    if (!ctx || !out || !req) return PD_EINVAL;
+    *out = nullptr;
+    // Coordinates arrive at execute time; validate the rest on the host.
+    pd_request r = *req;
+    static const double zero3[3] = {0, 0, 0};
+    std::vector<double> dummy;
+    const uint64_t nf = r.n_frames ? r.n_frames : 1;
+    if (!r.xyz) {
+        dummy.assign(static_cast<size_t>(r.n_atoms) * 3 * nf, 0.0);
+        r.xyz = dummy.data();
+    }
+    (void)zero3;
+    std::string msg;
+    int rc = pd::validate_request(&r, false, msg);
+    if (rc) {
+        ctx->set_error(msg);
+        return rc;
+    }
+    std::lock_guard<std::mutex> g(ctx->solve_mu);
+    cudaSetDevice(ctx->device);
+    auto *p = new pd_plan();
+    rc = create_devplan(ctx, &r, r.species, r.hyd_weights, false, p->dp, ctx->stream);
+    if (rc == PD_OK) {
+        cudaError_t e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) rc = cuda_fail(ctx, e, "pd_plan_create");
+    }
+    if (rc) {
+        free_devplan(ctx, p->dp, ctx->stream);
+        delete p;
+        return rc;
+    }
+    *out = p;
+    return PD_OK;
+}
+
+int pd_plan_execute(pd_ctx *ctx, pd_plan *plan, const double *xyz_dev, double *out_terms_dev,
+                    void *stream) {
+    if (!ctx || !plan || !xyz_dev || !out_terms_dev) return PD_EINVAL;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    cudaSetDevice(ctx->device);
+    plan->dp.xyz_dev = xyz_dev;
+    if (!plan->profiling) return run_devplan(ctx, plan->dp, out_terms_dev, st);
+    std::pair<cudaEvent_t, cudaEvent_t> ev{nullptr, nullptr};
+    PD_CUDA(ctx, cudaEventCreate(&ev.first));
+    PD_CUDA(ctx, cudaEventCreate(&ev.second));
+    plan->pair_events.push_back(ev);
+    return run_devplan(ctx, plan->dp, out_terms_dev, st, &plan->pair_events.back());
+}
+
+int pd_plan_set_profiling(pd_ctx *ctx, pd_plan *plan, int enable) {
+    if (!ctx || !plan) return PD_EINVAL;
+    cudaSetDevice(ctx->device);
+    for (auto &e : plan->pair_events) {
+        cudaEventSynchronize(e.second);
+        cudaEventDestroy(e.first);
+        cudaEventDestroy(e.second);
+    }
+    plan->pair_events.clear();
+    plan->profiling = enable != 0;
+    return PD_OK;
+}
+
+int pd_plan_pair_kernel_ms(pd_ctx *ctx, pd_plan *plan, double *total_ms, uint64_t *n_launches) {
+    if (!ctx || !plan) return PD_EINVAL;
+    cudaSetDevice(ctx->device);
+    double tot = 0.0;
+    for (auto &e : plan->pair_events) {
+        cudaError_t err = cudaEventSynchronize(e.second);
+        if (err != cudaSuccess) return cuda_fail(ctx, err, "pd_plan_pair_kernel_ms");
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, e.first, e.second);
+        tot += ms;
+    }
+    if (total_ms) *total_ms = tot;
+    if (n_launches) *n_launches = plan->pair_events.size();
+    return PD_OK;
+}
+
+int pd_plan_execute_host(pd_ctx *ctx, pd_plan *plan, const double *xyz_host, double *out_terms) {
+    if (!ctx || !plan || !xyz_host || !out_terms) return PD_EINVAL;
+    std::lock_guard<std::mutex> g(ctx->solve_mu);
+    cudaSetDevice(ctx->device);
+    const Plan &P = plan->dp.P;
+    const size_t nx = static_cast<size_t>(P.n_atoms) * 3 * P.n_frames;
+    for (size_t i = 0; i < nx; ++i)
+        if (!std::isfinite(xyz_host[i])) {
+            ctx->set_error("non-finite coordinate at index " + std::to_string(i));
+            return PD_EINVAL;
+        }
+    double *xyz_dev = nullptr;
+    PD_CUDA(ctx, cudaMallocFromPoolAsync(reinterpret_cast<void **>(&xyz_dev), nx * 8, ctx->pool, ctx->stream));
+    cudaMemcpyAsync(xyz_dev, xyz_host, nx * 8, cudaMemcpyHostToDevice, ctx->stream);
+    plan->dp.xyz_dev = xyz_dev;
+    int rc = run_devplan(ctx, plan->dp, nullptr, ctx->stream);
+    if (rc == PD_OK) {
+        cudaError_t e = cudaMemcpyAsync(out_terms, plan->dp.dptr<double>(plan->dp.L.out),
+                                        static_cast<size_t>(6) * P.nq * 8,
+                                        cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) rc = cuda_fail(ctx, e, "pd_plan_execute_host");
+    }
+    cudaFreeAsync(xyz_dev, ctx->stream);
+    cudaStreamSynchronize(ctx->stream);
+    return rc;
+}
+
+void pd_plan_destroy(pd_ctx *ctx, pd_plan *plan) {
+    if (!ctx || !plan) return;
+    pd_plan_set_profiling(ctx, plan, 0);
+    std::lock_guard<std::mutex> g(ctx->solve_mu);
+    cudaSetDevice(ctx->device);
+    // Executions may be in flight on caller streams.
+    cudaDeviceSynchronize();
+    free_devplan(ctx, plan->dp, ctx->stream);
+    cudaStreamSynchronize(ctx->stream);
+    delete plan;
+}
+
+int pd_plan_info(const pd_plan *plan, uint32_t *q_block, uint32_t *j_chunk, uint64_t *n_tiles,
+                 uint64_t *device_bytes, uint64_t *upload_bytes) {
+    if (!plan) return PD_EINVAL;
+    if (upload_bytes) *upload_bytes = plan->dp.L.upload_bytes;
+    if (q_block) *q_block = static_cast<uint32_t>(plan->dp.P.tun.K);
+    if (j_chunk) *j_chunk = static_cast<uint32_t>(plan->dp.P.tun.TJ);
+    if (n_tiles) *n_tiles = plan->dp.P.jobs.size();
+    if (device_bytes) *device_bytes = plan->dp.L.total;
+    return PD_OK;
+}
+
+int pd_submit(pd_ctx *ctx, const pd_request *req, uint64_t *ticket) {
+    if (!ctx || !ticket) return PD_EINVAL;
+    std::string msg;
+    int rc = pd::validate_request(req, false, msg);
+    if (rc) {
+        ctx->set_error(msg);
+        return rc;
+    }
+    auto t = std::make_shared<PdTicket>();
+    const uint64_t n = req->n_atoms, nq = req->nq, S = req->n_species;
+    const uint64_t nf = req->n_frames ? req->n_frames : 1;
+    t->xyz.assign(req->xyz, req->xyz + n * 3 * nf);
+    t->species.assign(req->species, req->species + n);
+    t->ffA.assign(req->ff_atoms, req->ff_atoms + S * nq);
+    if (req->ff_excluded) t->ffC.assign(req->ff_excluded, req->ff_excluded + S * nq);
+    if (req->hyd_weights) {
+        t->hw.assign(req->hyd_weights, req->hyd_weights + n);
+        t->ffW.assign(req->ff_water, req->ff_water + nq);
+    }
+    if (req->frame_weights) t->fw.assign(req->frame_weights, req->frame_weights + nf);
+    t->req = *req;
+    t->req.xyz = t->xyz.data();
+    t->req.species = t->species.data();
+    t->req.ff_atoms = t->ffA.data();
+    t->req.ff_excluded = req->ff_excluded ? t->ffC.data() : nullptr;
+    t->req.hyd_weights = req->hyd_weights ? t->hw.data() : nullptr;
+    t->req.ff_water = req->hyd_weights ? t->ffW.data() : nullptr;
+    t->req.frame_weights = req->frame_weights ? t->fw.data() : nullptr;
+    t->t_submit = now_s();
+    {
+        std::lock_guard<std::mutex> lk(ctx->qmu);
+        if (!ctx->worker_started) {
+            ctx->worker = std::thread(worker_main, ctx);
+            ctx->worker_started = true;
+        }
+        t->id = ctx->next_ticket++;
+        ctx->tickets[t->id] = t;
+        ctx->pending.push_back(t->id);
+        *ticket = t->id;
+    }
+    ctx->qcv.notify_all();
+    return PD_OK;
+}
+
+int pd_poll(pd_ctx *ctx, uint64_t ticket) {
+    if (!ctx) return PD_EINVAL;
+    std::lock_guard<std::mutex> lk(ctx->qmu);
+    auto it = ctx->tickets.find(ticket);
+    if (it == ctx->tickets.end()) return PD_ENOTFOUND;
+    const int s = it->second->status;
+    return s == 0 ? 1 : (s == 1 ? 0 : s);
+}
+
+int pd_wait(pd_ctx *ctx, uint64_t ticket, int timeout_ms, double *out_terms) {
+    if (!ctx) return PD_EINVAL;
+    std::unique_lock<std::mutex> lk(ctx->qmu);
+    auto it = ctx->tickets.find(ticket);
+    if (it == ctx->tickets.end()) {
+        ctx->set_error("unknown ticket " + std::to_string(ticket));
+        return PD_ENOTFOUND;
+    }
+    auto t = it->second;
+    auto pred = [&] { return t->status != 1; };
+    if (timeout_ms < 0)
+        ctx->done_cv.wait(lk, pred);
+    else if (!ctx->done_cv.wait_for(lk, std::chrono::milliseconds(timeout_ms), pred)) {
+        ctx->set_error("ticket " + std::to_string(ticket) + " still running");
+        return PD_ETIMEOUT;
+    }
+    if (t->status < 0) {
+        ctx->set_error(t->err.empty() ? "request failed" : t->err);
+        return t->status;
+    }
+    if (out_terms) {
+        if (t->taken) {
+            ctx->set_error("the result of ticket " + std::to_string(ticket) + " was already taken");
+            return PD_EINVAL;
+        }
+        std::memcpy(out_terms, t->result.data(), t->result.size() * 8);
+        t->result = {};
+        t->result.shrink_to_fit();
+        t->taken = true;
+    }
+    return PD_OK;
+}
+
+int pd_cancel(pd_ctx *ctx, uint64_t ticket) {
+    if (!ctx) return PD_EINVAL;
+    {
+        std::lock_guard<std::mutex> lk(ctx->qmu);
+        auto it = ctx->tickets.find(ticket);
+        if (it == ctx->tickets.end()) return PD_ENOTFOUND;
+        if (it->second->status == 1) it->second->canceled = true;
+    }
+    ctx->qcv.notify_all();
+    return PD_OK;
+}
+
+int pd_ticket_times(pd_ctx *ctx, uint64_t ticket, double *t_submit, double *t_admit,
+                    double *t_done) {
+    if (!ctx) return PD_EINVAL;
+    std::lock_guard<std::mutex> lk(ctx->qmu);
+    auto it = ctx->tickets.find(ticket);
+    if (it == ctx->tickets.end()) return PD_ENOTFOUND;
+    if (t_submit) *t_submit = it->second->t_submit;
+    if (t_admit) *t_admit = it->second->t_admit;
+    if (t_done) *t_done = it->second->t_done;
+    return PD_OK;
+}
+
+int pd_combine(const double *terms, uint64_t nq, double vs, double c, double *total) {
+    if (!terms || !total) return PD_EINVAL;
+    for (uint64_t k = 0; k < nq; ++k) {
+        // DebyeTerms::combine (src/debye.rs:187-194), same operation order.
+        total[k] = terms[k] + vs * vs * terms[nq + k] + c * c * terms[2 * nq + k] -
+                   2.0 * vs * terms[3 * nq + k] + 2.0 * c * terms[4 * nq + k] -
+                   2.0 * vs * c * terms[5 * nq + k];
+    }
+    return PD_OK;
+}
+
+int pd_get_tuning(pd_ctx *ctx, uint64_t n_atoms, uint64_t nq, uint32_t precision,
+                  uint32_t *q_block, uint32_t *j_chunk) {
+    Tuning t = tuning_for(ctx, static_cast<int64_t>(n_atoms), static_cast<int64_t>(nq),
+                          static_cast<int>(precision));
+    if (q_block) *q_block = static_cast<uint32_t>(t.K);
+    if (j_chunk) *j_chunk = static_cast<uint32_t>(t.TJ);
+    return PD_OK;
+}
+
+int pd_set_tuning(pd_ctx *ctx, uint64_t n_atoms, uint64_t nq, uint32_t precision, uint32_t q_block,
+                  uint32_t j_chunk) {
+    if (!ctx) return PD_EINVAL;
+    if (!pd::valid_q_block(static_cast<int>(precision), static_cast<int>(q_block)) ||
+        j_chunk < 32 || j_chunk % 32 != 0) {
+        ctx->set_error("invalid tuning");
+        return PD_EINVAL;
+    }
+    const int nb = static_cast<int>(std::floor(std::log2(static_cast<double>(std::max<uint64_t>(n_atoms, 1)))));
+    const int qb = static_cast<int>(std::floor(std::log2(static_cast<double>(std::max<uint64_t>(nq, 1)))));
+    std::lock_guard<std::mutex> g(ctx->mu);
+    Tuning t;
+    t.K = static_cast<int>(q_block);
+    t.TJ = static_cast<int>(j_chunk);
+    ctx->tuning[std::make_tuple(static_cast<int>(precision), nb, qb)] = t;
+    return PD_OK;
+}
+
+int pd_autotune(pd_ctx *ctx, uint64_t n_atoms, uint64_t nq, uint32_t precision) {
+    if (!ctx || n_atoms < 2 || nq < 1) return PD_EINVAL;
+    // Synthetic globule of the bucket's size: uniform in a sphere at the
+    // density of a protein (≈ 12 Å³ per atom), four species.
+    std::mt19937_64 rng(12345);
+    std::uniform_real_distribution<double> U(-1.0, 1.0);
+    const double R = std::cbrt(12.0 * static_cast<double>(n_atoms) * 3.0 / (4.0 * M_PI));
+    std::vector<double> xyz(n_atoms * 3);
+    std::vector<uint32_t> sp(n_atoms);
+    for (uint64_t i = 0; i < n_atoms; ++i) {
+        double x, y, z;
+        do {
+            x = U(rng);
+            y = U(rng);
+            z = U(rng);
+        } while (x * x + y * y + z * z > 1.0);
+        xyz[3 * i] = R * x;
+        xyz[3 * i + 1] = R * y;
+        xyz[3 * i + 2] = R * z;
+        sp[i] = static_cast<uint32_t>(i % 4);
+    }
+    std::vector<double> ff(4 * nq, 1.0);
+    pd_request rq{};
+    rq.n_atoms = n_atoms;
+    rq.xyz = xyz.data();
+    rq.species = sp.data();
+    rq.n_species = 4;
+    rq.precision = precision;
+    rq.ff_atoms = ff.data();
+    rq.qmin = 0.0;
+    rq.qmax = 0.5;
+    rq.nq = nq;
+    std::vector<int> Ks = precision == PD_FP64 ? std::vector<int>{16, 32}
+                                               : std::vector<int>{32, 64, 96, 128};
+    std::vector<int> TJs = {512, 1024, 2048, 4096, 8192};
+    double best = 1e300;
+    Tuning best_t = pd::default_tuning(static_cast<int64_t>(n_atoms), static_cast<int64_t>(nq),
+                                       static_cast<int>(precision));
+    cudaSetDevice(ctx->device);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    double *xyz_dev = nullptr, *out_dev = nullptr;
+    cudaMalloc(reinterpret_cast<void **>(&xyz_dev), xyz.size() * 8);
+    cudaMalloc(reinterpret_cast<void **>(&out_dev), 6 * nq * 8);
+    cudaMemcpy(xyz_dev, xyz.data(), xyz.size() * 8, cudaMemcpyHostToDevice);
+    for (int K : Ks) {
+        if (precision != PD_FP64 && nq <= 32 && K != 32) continue;
+        for (int TJ : TJs) {
+            if (TJ > static_cast<int>(2 * n_atoms) && TJ != TJs.front()) continue;
+            pd_set_tuning(ctx, n_atoms, nq, precision, K, TJ);
+            pd_plan *plan = nullptr;
+            if (pd_plan_create(ctx, &rq, &plan) != PD_OK) continue;
+            float ms = 0;
+            bool ok = pd_plan_execute(ctx, plan, xyz_dev, out_dev, ctx->stream) == PD_OK;
+            cudaEventRecord(e0, ctx->stream);
+            for (int rep = 0; rep < 2 && ok; ++rep)
+                ok = pd_plan_execute(ctx, plan, xyz_dev, out_dev, ctx->stream) == PD_OK;
+            cudaEventRecord(e1, ctx->stream);
+            if (cudaEventSynchronize(e1) != cudaSuccess) ok = false;
+            cudaEventElapsedTime(&ms, e0, e1);
+            pd_plan_destroy(ctx, plan);
+            if (ok && ms < best) {
+                best = ms;
+                best_t.K = K;
+                best_t.TJ = TJ;
+            }
+        }
+    }
+    cudaFree(xyz_dev);
+    cudaFree(out_dev);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return pd_set_tuning(ctx, n_atoms, nq, precision, best_t.K, best_t.TJ);
+}
+
+int pd_plan_inspect(pd_ctx *ctx, const pd_request *req, uint64_t *n_classes, uint64_t *n_padded,
+                    uint64_t *n_tiles, uint64_t *pairs_covered) {
+    std::string msg;
+    int rc = pd::validate_request(req, false, msg);
+    if (rc) {
+        if (ctx) ctx->set_error(msg);
+        return rc;
+    }
+    Tuning tun = tuning_for(ctx, static_cast<int64_t>(req->n_atoms), static_cast<int64_t>(req->nq),
+                            static_cast<int>(req->precision));
+    Plan P;
+    rc = pd::build_plan(req, req->species, req->hyd_weights, tun, P, msg, /*count_pairs=*/true);
+    if (rc) {
+        if (ctx) ctx->set_error(msg);
+        return rc;
+    }
+    if (n_classes) *n_classes = static_cast<uint64_t>(P.n_cls);
+    if (n_padded) *n_padded = static_cast<uint64_t>(P.n_pad);
+    if (n_tiles) *n_tiles = P.jobs.size();
+    if (pairs_covered) *pairs_covered = P.pairs_covered;
+    return PD_OK;
+}
+
+int pd_measure_fp32_peak(pd_ctx *ctx, double *tflops_ffma, double *tflops_ffma2) {
+    if (!ctx) return PD_EINVAL;
+    cudaSetDevice(ctx->device);
+    float *d = nullptr;
+    PD_CUDA(ctx, cudaMalloc(reinterpret_cast<void **>(&d), 4));
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    const int block = 256, grid = ctx->sm_count * 8, iters = 4096;
+    const double flops = 2.0 * 16 * 8 * static_cast<double>(iters) * block * grid;
+    for (int packed = 0; packed < 2; ++packed) {
+        pd::launch_ffma_probe(d, iters / 8, grid, block, packed != 0, ctx->stream);  // warm-up
+        cudaEventRecord(e0, ctx->stream);
+        pd::launch_ffma_probe(d, iters, grid, block, packed != 0, ctx->stream);
+        cudaEventRecord(e1, ctx->stream);
+        cudaError_t e = cudaEventSynchronize(e1);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "fp32 probe");
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        const double tf = flops * (packed ? 2.0 : 1.0) / (ms * 1e-3) / 1e12;
+        if (packed == 0 && tflops_ffma) *tflops_ffma = tf;
+        if (packed == 1 && tflops_ffma2) *tflops_ffma2 = tf;
+        ctx->launches += 2;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(d);
+    return PD_OK;
+}
+
+uint64_t pd_launch_count(pd_ctx *ctx) { return ctx ? ctx->launches.load() : 0; }
+
+}  // extern "C"

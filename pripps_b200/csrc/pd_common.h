@@ -1,0 +1,81 @@
+// Internal types shared by the host planner (pd_plan.cpp) and the device
+// kernels (pd_kernels.cu) of libpripps_debye.
+//
+// Data layout in HBM, per request:
+//   * atoms are re-ordered into "classes" (species, or species × hydration
+//     weight when few distinct weights exist) and each class is padded to a
+//     multiple of PD_GRANULE = 32 atoms, so that every warp-row of 32 i-atoms
+//     belongs to one class; padded atoms are inert (gvalid masks them);
+//   * coordinates are stored as float4 {x, y, z, w} (FP32 form) or double4
+//     (FP64 form), centred on the frame centroid; w carries the per-atom
+//     hydration weight in the weighted mode and is unused otherwise;
+//   * a tile ("job") is (frame, i-block of PD_IBLOCK atoms, contiguous j range
+//     of real atoms of ONE class, q-block of K grid points); it covers the
+//     pairs (i, j) with j > i;
+//   * each of the PD_WARPS warps of a tile writes its warp-reduced partial
+//     sums for the K q-points to its own FP64 slot; a second kernel adds the
+//     slots of every (class pair, q) in a fixed order, so the result does not
+//     depend on which SM ran which tile.
+#pragma once
+
+#include <cstdint>
+
+#ifndef __CUDACC__
+struct float4 { float x, y, z, w; };
+struct double4 { double x, y, z, w; };
+#else
+#include <cuda_runtime.h>
+#endif
+
+constexpr int PD_GRANULE = 32;                    // atoms per warp-row
+constexpr int PD_WARPS = 4;                       // warps per tile CTA
+constexpr int PD_THREADS = PD_GRANULE * PD_WARPS; // 128 threads
+constexpr int PD_IBLOCK = PD_THREADS;             // i-atoms per tile
+
+// Mode of the pair accumulation.
+//   PD_MODE_CLASS:    one accumulator, Σ sin(q r)/r per class pair; every
+//                     per-atom factor is a per-class constant.
+//   PD_MODE_WEIGHTED: two accumulators, Σ sin(q r)/r and Σ w_j sin(q r)/r, for
+//                     hydration weights that vary within a species.
+enum PdMode : int32_t { PD_MODE_CLASS = 0, PD_MODE_WEIGHTED = 1 };
+
+struct PdJob {
+    int32_t req;    // request index within the launch
+    int32_t frame;  // frame of the request
+    int32_t i0;     // first padded i index (multiple of PD_IBLOCK)
+    int32_t j0, j1; // padded j range [j0, j1): real atoms of one class
+    int32_t qb;     // q-block index
+    int64_t slot;   // first of the PD_WARPS output slots of this tile
+};
+static_assert(sizeof(PdJob) == 32, "PdJob layout");
+
+// Per-request descriptor read by the pair kernels.
+struct PdReqDev {
+    const float4 *atoms32;    // [n_frames][n_pad] (FP32 form)
+    const double4 *atoms64;   // [n_frames][n_pad] (FP64 form)
+    const int32_t *gvalid;    // [n_pad / 32] valid atoms per granule
+    const double *qv;         // [nq] grid (FP64 form reads it directly)
+    double *slots;            // [n_slots][nv][K]
+    double qmin, dq;          // grid origin and step
+    int32_t n_pad;
+    int32_t nq;
+    int32_t K;
+    int32_t mode;
+};
+
+// Per-class constants for the combine kernel.
+struct PdClassDev {
+    int32_t species;
+    int32_t pad;
+    double n;   // atoms in the class
+    double w;   // hydration weight (class mode)
+    double w1;  // Σ w_i over the class (weighted mode)
+    double w2;  // Σ w_i² over the class (weighted mode)
+};
+
+// Per-class-pair constants: classes (a <= b) and the q = 0 pair sums
+// (sinc = 1 for every pair): count, Σ w_i, Σ w_j, Σ w_i w_j.
+struct PdPairDev {
+    int32_t a, b;
+    double q0[4];
+};

@@ -1,0 +1,36 @@
+// Host-callable launchers of the device kernels (pd_kernels.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "pd_common.h"
+
+namespace pd {
+
+bool valid_q_block(int precision, int K);
+int pairs_blocks_per_sm(int precision, int K, int mode);
+
+// n_jobs points to the tile count in device memory (read once per CTA).
+cudaError_t launch_pairs(int precision, int K, int mode, const PdJob *jobs, const int *n_jobs,
+                         const PdReqDev *reqs, int *counter, int grid, cudaStream_t st);
+cudaError_t launch_centroid(const double *xyz, int64_t n_atoms, int n_frames, double *centroid,
+                            cudaStream_t st);
+cudaError_t launch_pack(const double *xyz, const double *weights, const int32_t *perm,
+                        const double *centroid, int64_t n_atoms, int32_t n_pad, int32_t n_frames,
+                        float4 *out32, double4 *out64, cudaStream_t st);
+cudaError_t launch_reduce(const double *slots, const int64_t *lptr, const int64_t *lidx,
+                          const PdPairDev *pairs, const double *qv, int32_t n_pairs, int32_t nq,
+                          int32_t K, int32_t nv, int32_t n_frames, int64_t slots_per_frame,
+                          double *pairsum, cudaStream_t st);
+cudaError_t launch_combine(const double *pairsum, const PdClassDev *cls, const PdPairDev *pairs,
+                           int32_t n_cls, int32_t n_pairs, int32_t nq, int32_t nv,
+                           int32_t n_frames, const double *ffA, const double *ffC,
+                           const double *ffW, double *terms, cudaStream_t st);
+cudaError_t launch_frame_mean(const double *terms, const double *fw, int32_t n_frames, int32_t nq,
+                              double *out, cudaStream_t st);
+cudaError_t launch_ffma_probe(float *out, int iters, int grid, int block, bool packed,
+                              cudaStream_t st);
+
+}  // namespace pd

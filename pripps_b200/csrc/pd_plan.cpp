@@ -1,0 +1,396 @@
+// Host planner of the Debye backend: classes, padded layout, tiles and the
+// fixed-order reduction lists (see pd_common.h for the layout).
+#include "pd_plan.h"
+
+#include <algorithm>
+#include <cmath>
+#include <map>
+#include <numeric>
+#include <utility>
+
+#include "pd_kernels.h"
+
+namespace pd {
+
+uint64_t Plan::device_bytes() const {
+    const uint64_t atoms = static_cast<uint64_t>(n_pad) * n_frames *
+                           (precision == PD_FP64 ? sizeof(double4) : sizeof(float4));
+    const uint64_t xyz_in = static_cast<uint64_t>(n_atoms) * 3 * n_frames * sizeof(double);
+    const uint64_t tables = static_cast<uint64_t>(n_species) * nq * 2 * sizeof(double) +
+                            static_cast<uint64_t>(nq) * 2 * sizeof(double) +
+                            static_cast<uint64_t>(n_atoms) * sizeof(double);
+    const uint64_t layout = static_cast<uint64_t>(n_pad) * sizeof(int32_t) +
+                            gvalid.size() * sizeof(int32_t) +
+                            cls.size() * sizeof(PdClassDev) + pairs.size() * sizeof(PdPairDev);
+    const uint64_t jb = jobs.size() * sizeof(PdJob);
+    const uint64_t slots = static_cast<uint64_t>(slots_per_frame) * n_frames * nv * tun.K *
+                           sizeof(double);
+    const uint64_t lists = (lptr.size() + lidx.size()) * sizeof(int64_t);
+    const uint64_t sums = static_cast<uint64_t>(n_frames) * nv * n_pairs * nq * sizeof(double);
+    const uint64_t terms = static_cast<uint64_t>(n_frames + 1) * 6 * nq * sizeof(double);
+    const uint64_t misc = static_cast<uint64_t>(n_frames) * 4 * sizeof(double) + 4096;
+    return atoms + xyz_in + tables + layout + jb + slots + lists + sums + terms + misc;
+}
+
+int validate_request(const pd_request *req, bool device_pointers, std::string &msg) {
+    if (!req) {
+        msg = "request is NULL";
+        return PD_EINVAL;
+    }
+    if (req->n_atoms == 0) {
+        msg = "n_atoms must be >= 1";
+        return PD_EINVAL;
+    }
+    if (req->n_atoms > (1ull << 30)) {
+        msg = "n_atoms exceeds 2^30";
+        return PD_EINVAL;
+    }
+    if (req->nq == 0 || req->nq > (1ull << 24)) {
+        msg = "nq must be in [1, 2^24]";
+        return PD_EINVAL;
+    }
+    if (req->n_species == 0) {
+        msg = "n_species must be >= 1";
+        return PD_EINVAL;
+    }
+    if (req->precision != PD_FP32_FP64RED && req->precision != PD_FP64) {
+        msg = "precision must be PD_FP32_FP64RED or PD_FP64";
+        return PD_EINVAL;
+    }
+    if (!req->xyz || !req->species || !req->ff_atoms) {
+        msg = "xyz, species and ff_atoms are required";
+        return PD_EINVAL;
+    }
+    if (req->hyd_weights && !req->ff_water) {
+        msg = "ff_water is required when hyd_weights is given";
+        return PD_EINVAL;
+    }
+    if (req->flags != 0 || req->reserved != 0) {
+        msg = "flags and reserved must be 0";
+        return PD_EINVAL;
+    }
+    if (!std::isfinite(req->qmin) || !std::isfinite(req->qmax) || req->qmin < 0.0 ||
+        req->qmax < req->qmin) {
+        msg = "q range must satisfy 0 <= qmin <= qmax (finite)";
+        return PD_EINVAL;
+    }
+    const uint64_t nf = req->n_frames ? req->n_frames : 1;
+    if (nf > (1u << 20)) {
+        msg = "n_frames exceeds 2^20";
+        return PD_EINVAL;
+    }
+    if (device_pointers) return PD_OK;
+    // Host buffers: check the values the planner and the kernels rely on.
+    const uint64_t n = req->n_atoms;
+    for (uint64_t i = 0; i < n; ++i) {
+        if (req->species[i] >= req->n_species) {
+            msg = "species id " + std::to_string(req->species[i]) + " at atom " +
+                  std::to_string(i) + " is >= n_species";
+            return PD_EINVAL;
+        }
+    }
+    for (uint64_t i = 0; i < n * 3 * nf; ++i) {
+        if (!std::isfinite(req->xyz[i])) {
+            msg = "non-finite coordinate at index " + std::to_string(i);
+            return PD_EINVAL;
+        }
+    }
+    const uint64_t nt = static_cast<uint64_t>(req->n_species) * req->nq;
+    for (uint64_t i = 0; i < nt; ++i) {
+        if (!std::isfinite(req->ff_atoms[i]) ||
+            (req->ff_excluded && !std::isfinite(req->ff_excluded[i]))) {
+            msg = "non-finite form-factor table entry";
+            return PD_EINVAL;
+        }
+    }
+    if (req->hyd_weights) {
+        for (uint64_t i = 0; i < n; ++i)
+            if (!std::isfinite(req->hyd_weights[i])) {
+                msg = "non-finite hydration weight";
+                return PD_EINVAL;
+            }
+        for (uint64_t i = 0; i < req->nq; ++i)
+            if (!std::isfinite(req->ff_water[i])) {
+                msg = "non-finite water form factor";
+                return PD_EINVAL;
+            }
+    }
+    if (req->frame_weights) {
+        double s = 0.0;
+        for (uint64_t f = 0; f < nf; ++f) {
+            if (!std::isfinite(req->frame_weights[f])) {
+                msg = "non-finite frame weight";
+                return PD_EINVAL;
+            }
+            s += req->frame_weights[f];
+        }
+        // trajectory_average rejects a sum that is zero or not normal
+        // (src/trajectory.rs:234-238).
+        if (!std::isnormal(std::fabs(s))) {
+            msg = "frame weights sum to zero or a non-normal value; cannot normalize";
+            return PD_EINVAL;
+        }
+    }
+    return PD_OK;
+}
+
+static int next_pow2(int64_t v) {
+    int p = 1;
+    while (p < v && p < (1 << 30)) p <<= 1;
+    return p;
+}
+
+Tuning default_tuning(int64_t n_atoms, int64_t nq, int precision) {
+    Tuning t;
+    if (precision == PD_FP64) {
+        t.K = 32;
+        t.TJ = std::clamp(next_pow2(n_atoms / 16), 256, 4096);
+        return t;
+    }
+    // Longest block that wastes at most ~12 % of a short q grid.
+    t.K = 128;
+    for (int k : {128, 96, 64}) {
+        const int64_t nb = (nq + k - 1) / k;
+        if (nb * k - nq <= std::max<int64_t>(nq / 8, 0) || k == 64) {
+            t.K = k;
+            break;
+        }
+    }
+    if (nq <= 32) t.K = 32;
+    t.TJ = std::clamp(next_pow2(n_atoms / 8), 512, 8192);
+    return t;
+}
+
+int build_plan(const pd_request *req, const uint32_t *species, const double *w,
+               const Tuning &tun, Plan &P, std::string &msg, bool count_pairs) {
+    P = Plan();
+    P.n_atoms = static_cast<int64_t>(req->n_atoms);
+    P.nq = static_cast<int32_t>(req->nq);
+    P.n_frames = static_cast<int32_t>(req->n_frames ? req->n_frames : 1);
+    P.n_species = static_cast<int32_t>(req->n_species);
+    P.precision = static_cast<int>(req->precision);
+    P.has_exc = req->ff_excluded != nullptr;
+    P.has_hyd = req->hyd_weights != nullptr;
+    P.tun = tun;
+    if (!valid_q_block(P.precision, tun.K) || tun.TJ < 32 || tun.TJ % 32 != 0) {
+        msg = "invalid tuning (q block " + std::to_string(tun.K) + ", j chunk " +
+              std::to_string(tun.TJ) + ")";
+        return PD_EINVAL;
+    }
+    P.qmin = req->qmin;
+    P.qmax = req->qmax;
+    // Grid exactly as linear_q_values (src/q_sampler.rs:24-29).
+    const double denom = static_cast<double>(P.nq > 1 ? P.nq - 1 : 1);
+    P.qv.resize(P.nq);
+    for (int k = 0; k < P.nq; ++k)
+        P.qv[k] = P.qmin + (P.qmax - P.qmin) * static_cast<double>(k) / denom;
+    P.dq = (P.qmax - P.qmin) / denom;
+
+    const int64_t n = P.n_atoms;
+    // ---- classes: species, or (species, weight) while few distinct weights
+    std::map<std::pair<uint32_t, double>, int> keys;
+    bool by_weight = P.has_hyd;
+    if (by_weight) {
+        for (int64_t i = 0; i < n; ++i) {
+            keys.emplace(std::make_pair(species[i], w[i]), 0);
+            if (static_cast<int>(keys.size()) > PD_MAX_CLASSES) {
+                by_weight = false;
+                break;
+            }
+        }
+    }
+    if (!by_weight) {
+        keys.clear();
+        for (int64_t i = 0; i < n; ++i) keys.emplace(std::make_pair(species[i], 0.0), 0);
+    }
+    P.mode = (P.has_hyd && !by_weight) ? PD_MODE_WEIGHTED : PD_MODE_CLASS;
+    P.nv = P.mode == PD_MODE_WEIGHTED ? 4 : 1;
+    // Two accumulators per q: longer q blocks than 64 spill registers.
+    if (P.mode == PD_MODE_WEIGHTED && P.precision == PD_FP32_FP64RED && P.tun.K > 64)
+        P.tun.K = 64;
+    int c = 0;
+    for (auto &kv : keys) kv.second = c++;
+    P.n_cls = c;
+    P.cls.assign(c, PdClassDev{});
+    {
+        int ci = 0;
+        for (auto &kv : keys) {
+            P.cls[ci].species = static_cast<int32_t>(kv.first.first);
+            P.cls[ci].w = kv.first.second;
+            ++ci;
+        }
+    }
+    std::vector<int32_t> atom_cls(n);
+    std::vector<std::vector<int32_t>> members(c);
+    for (int64_t i = 0; i < n; ++i) {
+        const double wk = by_weight ? w[i] : 0.0;
+        const int k = keys.at(std::make_pair(species[i], wk));
+        atom_cls[i] = k;
+        members[k].push_back(static_cast<int32_t>(i));
+    }
+    // ---- padded layout
+    P.cls_start.assign(c, 0);
+    int64_t cur = 0;
+    for (int k = 0; k < c; ++k) {
+        P.cls_start[k] = static_cast<int32_t>(cur);
+        const int64_t nk = static_cast<int64_t>(members[k].size());
+        cur += (nk + PD_GRANULE - 1) / PD_GRANULE * PD_GRANULE;
+    }
+    cur = (cur + PD_IBLOCK - 1) / PD_IBLOCK * PD_IBLOCK;
+    if (cur > (int64_t{1} << 31) - PD_IBLOCK) {
+        msg = "padded atom count overflows";
+        return PD_EINVAL;
+    }
+    P.n_pad = static_cast<int32_t>(cur);
+    P.perm.assign(P.n_pad, -1);
+    const int ng = P.n_pad / PD_GRANULE;
+    P.gvalid.assign(ng, 0);
+    P.gclass.assign(ng, -1);
+    for (int k = 0; k < c; ++k) {
+        const int64_t nk = static_cast<int64_t>(members[k].size());
+        double s1 = 0, s2 = 0;
+        for (int64_t r = 0; r < nk; ++r) {
+            const int32_t src = members[k][r];
+            P.perm[P.cls_start[k] + r] = src;
+            if (P.has_hyd) {
+                s1 += w[src];
+                s2 += w[src] * w[src];
+            }
+        }
+        P.cls[k].n = static_cast<double>(nk);
+        P.cls[k].w1 = s1;
+        P.cls[k].w2 = s2;
+        for (int64_t g = 0; g < (nk + PD_GRANULE - 1) / PD_GRANULE; ++g) {
+            const int gi = P.cls_start[k] / PD_GRANULE + static_cast<int>(g);
+            P.gclass[gi] = k;
+            P.gvalid[gi] = static_cast<int32_t>(std::min<int64_t>(PD_GRANULE, nk - g * PD_GRANULE));
+        }
+    }
+    // ---- class pairs (a <= b) and their exact q = 0 sums
+    std::vector<int> pair_index(static_cast<size_t>(c) * c, -1);
+    for (int a = 0; a < c; ++a)
+        for (int b = a; b < c; ++b) {
+            PdPairDev pd{};
+            pd.a = a;
+            pd.b = b;
+            const double na = P.cls[a].n, nb = P.cls[b].n;
+            if (a != b) {
+                pd.q0[0] = na * nb;
+                pd.q0[1] = P.cls[a].w1 * nb;
+                pd.q0[2] = na * P.cls[b].w1;
+                pd.q0[3] = P.cls[a].w1 * P.cls[b].w1;
+            } else {
+                pd.q0[0] = na * (na - 1.0) / 2.0;
+                // Σ_{i<j} w_i and Σ_{i<j} w_j in padded order within the class.
+                double ti = 0, tj = 0, tij = 0, pre = 0;
+                const int64_t nk = static_cast<int64_t>(members[a].size());
+                for (int64_t r = 0; r < nk; ++r) {
+                    const double wr = P.has_hyd ? w[members[a][r]] : 0.0;
+                    ti += wr * static_cast<double>(nk - 1 - r);
+                    tj += wr * static_cast<double>(r);
+                    tij += wr * pre;
+                    pre += wr;
+                }
+                pd.q0[1] = ti;
+                pd.q0[2] = tj;
+                pd.q0[3] = tij;
+            }
+            pair_index[a * c + b] = static_cast<int>(P.pairs.size());
+            P.pairs.push_back(pd);
+        }
+    P.n_pairs = static_cast<int>(P.pairs.size());
+
+    // ---- tiles of one frame, in creation order
+    const int K = P.tun.K, TJ = P.tun.TJ;
+    P.nqb = (P.nq + K - 1) / K;
+    struct Tile {
+        int32_t i0, j0, j1, cls;
+    };
+    std::vector<Tile> tiles;
+    const int nblocks = P.n_pad / PD_IBLOCK;
+    for (int ib = 0; ib < nblocks; ++ib) {
+        const int32_t i0 = ib * PD_IBLOCK;
+        int min_cls = -1;
+        for (int wv = 0; wv < PD_WARPS; ++wv) {
+            const int g = ib * PD_WARPS + wv;
+            if (P.gvalid[g] > 0) {
+                min_cls = P.gclass[g];
+                break;
+            }
+        }
+        if (min_cls < 0) continue;
+        for (int k = min_cls; k < c; ++k) {
+            const int32_t cend = P.cls_start[k] + static_cast<int32_t>(members[k].size());
+            const int32_t s0 = std::max(i0, P.cls_start[k]);
+            if (cend - 1 <= i0) continue;  // no j > the block's first atom
+            for (int32_t j0 = s0; j0 < cend; j0 += TJ)
+                tiles.push_back(Tile{i0, j0, std::min(cend, j0 + TJ), k});
+        }
+    }
+    P.jobs_per_frame = static_cast<int64_t>(tiles.size()) * P.nqb;
+    P.slots_per_frame = P.jobs_per_frame * PD_WARPS;
+    if (P.jobs_per_frame * P.n_frames > (int64_t{1} << 31) - 1) {
+        msg = "too many tiles for one launch; use a larger j chunk";
+        return PD_EINVAL;
+    }
+    // Reduction lists: (pair, q-block) -> slots in creation order.
+    std::vector<std::vector<int64_t>> lists(static_cast<size_t>(P.n_pairs) * P.nqb);
+    std::vector<PdJob> frame_jobs;
+    frame_jobs.reserve(P.jobs_per_frame);
+    uint64_t covered = 0;
+    int64_t jl = 0;
+    for (const Tile &t : tiles) {
+        for (int qb = 0; qb < P.nqb; ++qb, ++jl) {
+            PdJob jb{};
+            jb.req = 0;
+            jb.frame = 0;
+            jb.i0 = t.i0;
+            jb.j0 = t.j0;
+            jb.j1 = t.j1;
+            jb.qb = qb;
+            jb.slot = jl * PD_WARPS;
+            frame_jobs.push_back(jb);
+            for (int wv = 0; wv < PD_WARPS; ++wv) {
+                const int g = t.i0 / PD_GRANULE + wv;
+                const int a = P.gclass[g];
+                if (a < 0 || P.gvalid[g] == 0 || a > t.cls) continue;
+                const int64_t ilo = static_cast<int64_t>(g) * PD_GRANULE;
+                const int64_t ihi = ilo + P.gvalid[g];  // exclusive
+                if (t.j1 - 1 <= ilo) continue;          // every j <= every i
+                lists[static_cast<size_t>(pair_index[a * c + t.cls]) * P.nqb + qb].push_back(
+                    jl * PD_WARPS + wv);
+                if (qb == 0 && count_pairs) {
+                    for (int64_t i = ilo; i < ihi; ++i) {
+                        const int64_t lo = std::max<int64_t>(t.j0, i + 1);
+                        if (t.j1 > lo) covered += static_cast<uint64_t>(t.j1 - lo);
+                    }
+                }
+            }
+        }
+    }
+    P.pairs_covered = covered;
+    P.lptr.assign(static_cast<size_t>(P.n_pairs) * P.nqb + 1, 0);
+    for (size_t e = 0; e < lists.size(); ++e) P.lptr[e + 1] = P.lptr[e] + lists[e].size();
+    P.lidx.reserve(P.lptr.back());
+    for (auto &l : lists) P.lidx.insert(P.lidx.end(), l.begin(), l.end());
+
+    // Execution order: longest tiles first (j length), stable; replicated
+    // per frame with frame-offset slots.
+    std::vector<int64_t> order(frame_jobs.size());
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int64_t x, int64_t y) {
+        return (frame_jobs[x].j1 - frame_jobs[x].j0) > (frame_jobs[y].j1 - frame_jobs[y].j0);
+    });
+    P.jobs.reserve(order.size() * P.n_frames);
+    for (int64_t o : order) {
+        for (int f = 0; f < P.n_frames; ++f) {
+            PdJob jb = frame_jobs[o];
+            jb.frame = f;
+            jb.slot += static_cast<int64_t>(f) * P.slots_per_frame;
+            P.jobs.push_back(jb);
+        }
+    }
+    return PD_OK;
+}
+
+}  // namespace pd

@@ -1,0 +1,71 @@
+// Host planner: turns a pd_request into the device layout and tile list.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "pd_common.h"
+#include "pripps_debye.h"
+
+namespace pd {
+
+// At most this many (species, hydration weight) classes use the one-
+// accumulator class mode; more distinct weights switch to the weighted mode.
+constexpr int PD_MAX_CLASSES = 48;
+
+struct Tuning {
+    int K = 64;     // q-block length
+    int TJ = 2048;  // j atoms per tile
+};
+
+struct Plan {
+    // request shape
+    int64_t n_atoms = 0;
+    int32_t nq = 0;
+    int32_t n_frames = 1;
+    int32_t n_species = 0;
+    int precision = 0;
+    bool has_exc = false, has_hyd = false;
+    int mode = PD_MODE_CLASS;
+    int nv = 1;  // values per slot entry: 1 (class) or 4 (weighted)
+    Tuning tun;
+    double qmin = 0, qmax = 0, dq = 0;
+    std::vector<double> qv;
+
+    // classes and layout
+    int n_cls = 0, n_pairs = 0;
+    std::vector<PdClassDev> cls;
+    std::vector<PdPairDev> pairs;
+    std::vector<int32_t> cls_start;  // padded start of each class region
+    int32_t n_pad = 0;
+    std::vector<int32_t> perm;    // [n_pad] source atom or -1
+    std::vector<int32_t> gvalid;  // [n_pad/32]
+    std::vector<int32_t> gclass;  // [n_pad/32] class or -1
+
+    // tiles (execution order) and the deterministic reduction lists
+    std::vector<PdJob> jobs;        // all frames
+    int64_t jobs_per_frame = 0;
+    int64_t slots_per_frame = 0;
+    int nqb = 0;
+    std::vector<int64_t> lptr;  // [n_pairs * nqb + 1]
+    std::vector<int64_t> lidx;  // slot indices within a frame
+    uint64_t pairs_covered = 0; // per frame, unordered pairs over all tiles
+
+    // device memory the plan needs, in bytes
+    uint64_t device_bytes() const;
+};
+
+// Validate a request; fills msg and returns a PD_E* code on failure.
+int validate_request(const pd_request *req, bool device_pointers, std::string &msg);
+
+// Default shape when no tuned entry exists.
+Tuning default_tuning(int64_t n_atoms, int64_t nq, int precision);
+
+// Build the plan from host-side species and weights (hyd may be NULL).
+// count_pairs fills Plan::pairs_covered (an O(N · tiles per block) host loop
+// that only pd_plan_inspect needs).
+int build_plan(const pd_request *req, const uint32_t *species_host, const double *weights_host,
+               const Tuning &tun, Plan &plan, std::string &msg, bool count_pairs = false);
+
+}  // namespace pd

@@ -1,0 +1,272 @@
+"""Debye scattering on the B200: the six cached profiles and what sits on them.
+
+Host-side mirror of the reference's Debye calculator (src/debye.rs), cached
+model (``DebyeModel``, src/debye.rs:138-174), library entry points
+(``Pripps.debye_model`` / ``Pripps.intensity``, src/lib.rs:287-303, 344-528)
+and trajectory averaging (src/trajectory.rs:167-251). The pair sum itself —
+the per-q body of ``build_model`` (src/debye.rs:90-130) — runs in
+libpripps_debye through ``pd_solve``; nothing here computes a pair term.
+
+``DebyeModel.intensity(volume_scale, contrast_density)`` recombines the six
+cached terms exactly as ``DebyeTerms::combine`` does (src/debye.rs:187-194),
+so fits and the one-shot path share one kernel result.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+from .errors import ValidationError
+from .formfactor import FormFactorMap, linear_q_values, read_formfactors
+from .solvent import SolventConfig, excluded_table, sasa_weights, water_table
+from .structure import Structure, structure_from_xyz
+
+TERM_NAMES = ("atoms", "excluded", "hydration", "atom_excluded", "atom_hydration",
+              "excluded_hydration")
+
+
+@dataclass
+class Contributions:
+    """Unscaled self profiles (src/lib.rs:113-121)."""
+    atoms: np.ndarray
+    excluded: np.ndarray
+    hydration: np.ndarray
+
+    def __eq__(self, other):
+        return (isinstance(other, Contributions) and np.array_equal(self.atoms, other.atoms)
+                and np.array_equal(self.excluded, other.excluded)
+                and np.array_equal(self.hydration, other.hydration))
+
+
+@dataclass
+class Intensity:
+    """I(q) on a q grid (src/lib.rs:89-109)."""
+    q: np.ndarray
+    total: np.ndarray
+    contributions: Optional[Contributions] = None
+
+
+def combine(terms: np.ndarray, volume_scale: float, contrast_density: float) -> np.ndarray:
+    """AA + v²CC + c²BB − 2v·AC + 2c·AB − 2vc·CB per q, in the reference's
+    operation order (src/debye.rs:187-194)."""
+    t = np.asarray(terms, dtype=np.float64)
+    v, c = float(volume_scale), float(contrast_density)
+    return (t[0] + v * v * t[1] + c * c * t[2] - 2.0 * v * t[3] + 2.0 * c * t[4]
+            - 2.0 * v * c * t[5])
+
+
+class DebyeModel:
+    """Cached six-profile Debye state for solvent fitting (src/debye.rs:138-174)."""
+
+    def __init__(self, q_values: np.ndarray, terms: np.ndarray):
+        self._q = np.asarray(q_values, dtype=np.float64)
+        self.terms = np.asarray(terms, dtype=np.float64).reshape(6, -1)
+
+    @property
+    def q_values(self) -> np.ndarray:
+        return self._q
+
+    def intensity(self, volume_scale: float = 1.0, contrast_density: float = 0.03) -> Intensity:
+        total = combine(self.terms, volume_scale, contrast_density)
+        return Intensity(self._q.copy(), total,
+                         Contributions(self.terms[0].copy(), self.terms[1].copy(),
+                                       self.terms[2].copy()))
+
+    def fit(self, q, intensity, sigma=None, *, method="nelder-mead", c1_points=151,
+            c2_points=101, c1_bounds=None, c2_bounds=None):
+        """Fit (volume_scale, contrast_density) to experimental data, as the
+        pyo3 ``cached_model!`` fit does (pripps-py/src/lib.rs:619-646)."""
+        from . import fit as _fit
+        exp = _fit.ExpData.from_arrays(q, intensity, [] if sigma is None else sigma)
+        c1b = _fit.DEFAULT_C1_BOUNDS if c1_bounds is None else tuple(c1_bounds)
+        c2b = _fit.DEFAULT_C2_BOUNDS if c2_bounds is None else tuple(c2_bounds)
+        ev = lambda c1, c2: self.intensity(c1, c2)
+        m = str(method).lower().replace("_", "-")
+        if m in ("nelder-mead", "neldermead"):
+            return _fit.fit_parameters_with_bounds(exp, ev, c1b, c2b)
+        if m == "grid":
+            return _fit.fit_parameters_grid_with_bounds(exp, ev, c1_points, c2_points, c1b, c2b)
+        raise ValidationError(f"unknown fit method {method!r}")
+
+
+# ------------------------------------------------------------------ requests
+@dataclass
+class DebyeRequest:
+    """Host arrays of one pd_request (see include/pripps_debye.h)."""
+    xyz: np.ndarray                    # [F, N, 3] or [N, 3] float64
+    species: np.ndarray                # [N] uint32, compact ids
+    ff_atoms: np.ndarray               # [S, nq]
+    ff_excluded: Optional[np.ndarray]  # [S, nq] or None
+    hyd_weights: Optional[np.ndarray]  # [N] or None
+    ff_water: Optional[np.ndarray]     # [nq] or None
+    qmin: float
+    qmax: float
+    nq: int
+    frame_weights: Optional[np.ndarray] = None
+    precision: str = "fp32"
+
+    def __post_init__(self):
+        self.xyz = np.ascontiguousarray(self.xyz, dtype=np.float64)
+        self.species = np.ascontiguousarray(self.species, dtype=np.uint32)
+        self.ff_atoms = np.ascontiguousarray(self.ff_atoms, dtype=np.float64)
+        if self.ff_excluded is not None:
+            self.ff_excluded = np.ascontiguousarray(self.ff_excluded, dtype=np.float64)
+        if self.hyd_weights is not None:
+            self.hyd_weights = np.ascontiguousarray(self.hyd_weights, dtype=np.float64)
+            self.ff_water = np.ascontiguousarray(self.ff_water, dtype=np.float64)
+        if self.frame_weights is not None:
+            self.frame_weights = np.ascontiguousarray(self.frame_weights, dtype=np.float64)
+
+    @property
+    def n_atoms(self) -> int:
+        return int(self.species.shape[0])
+
+    @property
+    def n_frames(self) -> int:
+        return int(self.xyz.shape[0]) if self.xyz.ndim == 3 else 1
+
+    def c_struct(self) -> _lib.PdRequest:
+        r = _lib.PdRequest()
+        r.n_atoms = self.n_atoms
+        r.xyz = _lib.dptr(self.xyz)
+        r.species = _lib.u32ptr(self.species)
+        r.n_species = int(self.ff_atoms.shape[0])
+        r.precision = _lib.PRECISIONS[self.precision]
+        r.ff_atoms = _lib.dptr(self.ff_atoms)
+        r.ff_excluded = _lib.dptr(self.ff_excluded)
+        r.hyd_weights = _lib.dptr(self.hyd_weights)
+        r.ff_water = _lib.dptr(self.ff_water)
+        r.qmin = float(self.qmin)
+        r.qmax = float(self.qmax)
+        r.nq = int(self.nq)
+        r.n_frames = self.n_frames if self.xyz.ndim == 3 else 0
+        r.frame_weights = _lib.dptr(self.frame_weights)
+        r.flags = 0
+        r.reserved = 0
+        return r
+
+
+def make_request(structure: Structure, formfactors: FormFactorMap, q_values: np.ndarray,
+                 qmin: float, qmax: float, solvent: Optional[SolventConfig],
+                 precision: str = "fp32", frames: Optional[np.ndarray] = None,
+                 frame_weights: Optional[np.ndarray] = None) -> DebyeRequest:
+    """Tabulate the per-species inputs of a solve on the host. Form factors are
+    evaluated only for the species the structure uses, so a QOutOfRange is
+    raised here exactly when the reference's formfactor_by_index would raise
+    it (src/formfactor.rs:520-544)."""
+    ids = structure.ids
+    used = np.unique(ids)
+    compact = np.searchsorted(used, ids).astype(np.uint32)
+    ffA = formfactors.table(used, q_values)
+    ffC = hw = ffW = None
+    if solvent is not None and solvent.is_active():
+        ffC = excluded_table(solvent.excluded, formfactors, used, q_values,
+                             solvent.bulk_electron_density)
+        if solvent.hydration.is_active():
+            hw = sasa_weights(solvent.hydration, formfactors, ids)
+            ffW = water_table(formfactors, q_values)
+    xyz = structure.pos if frames is None else np.asarray(frames, dtype=np.float64)
+    return DebyeRequest(xyz, compact, ffA, ffC, hw, ffW, qmin, qmax, len(q_values),
+                        frame_weights, precision)
+
+
+def solve(req: DebyeRequest, ctx: Optional[_lib.Context] = None) -> np.ndarray:
+    """Blocking pd_solve: the [6, nq] terms (frame-weighted mean for batches)."""
+    ctx = ctx or _lib.default_context()
+    out = np.empty((6, req.nq), dtype=np.float64)
+    r = req.c_struct()
+    _lib.check(_lib.lib().pd_solve(ctx.handle, C.byref(r), _lib.dptr(out)), ctx.handle)
+    return out
+
+
+# ------------------------------------------------------------------ facade
+class Pripps:
+    """High-level entry points over a form-factor table (src/lib.rs:212-250)."""
+
+    def __init__(self, formfactors: FormFactorMap, *, precision: str = "fp32",
+                 ctx: Optional[_lib.Context] = None):
+        if precision not in _lib.PRECISIONS:
+            raise ValidationError(f"precision must be one of {sorted(_lib.PRECISIONS)}")
+        self.formfactors = formfactors
+        self.precision = precision
+        self._ctx = ctx
+
+    @classmethod
+    def from_yaml(cls, path, **kw) -> "Pripps":
+        return cls(read_formfactors(path), **kw)
+
+    @property
+    def ctx(self) -> _lib.Context:
+        return self._ctx or _lib.default_context()
+
+    def _structure(self, structure) -> Structure:
+        if isinstance(structure, Structure):
+            return structure
+        return structure_from_xyz(structure, self.formfactors)
+
+    def debye_model(self, structure, qmin: float = 0.0, qmax: float = 0.5, nq: int = 100,
+                    solvent: Optional[SolventConfig] = None) -> DebyeModel:
+        """Cached six-profile model (src/lib.rs:287-303 → src/debye.rs:78-136).
+        Built on the unit basis; the knobs are applied in ``intensity``."""
+        s = self._structure(structure)
+        q = linear_q_values(qmin, qmax, nq)
+        cfg = solvent if solvent is not None else SolventConfig()
+        req = make_request(s, self.formfactors, q, qmin, qmax, cfg, self.precision)
+        return DebyeModel(q, solve(req, self.ctx))
+
+    def intensity(self, structure, qmin: float = 0.0, qmax: float = 0.5, nq: int = 100,
+                  solvent: Optional[SolventConfig] = None, *, frames=None, frame_weights=None,
+                  stride: int = 1) -> Intensity:
+        """One-shot Debye intensity (src/debye.rs:56-69). Vacuum returns AA with
+        no contributions; an active solvent builds the six terms and combines
+        them at the configured knobs. With ``frames`` ([F, N, 3] Å), the
+        weighted mean over frames[::stride] (src/trajectory.rs:167-251)."""
+        s = self._structure(structure)
+        q = linear_q_values(qmin, qmax, nq)
+        active = solvent if (solvent is not None and solvent.is_active()) else None
+        if frames is not None:
+            return self._trajectory(s, q, qmin, qmax, active, frames, frame_weights, stride)
+        req = make_request(s, self.formfactors, q, qmin, qmax, active, self.precision)
+        terms = solve(req, self.ctx)
+        if active is None:
+            return Intensity(q, terms[0].copy(), None)
+        model = DebyeModel(q, terms)
+        return model.intensity(active.excluded.effective_volume_scale(),
+                               active.hydration.effective_contrast_density())
+
+    def _trajectory(self, s, q, qmin, qmax, active, frames, frame_weights, stride):
+        frames = np.asarray(frames, dtype=np.float64)
+        if frames.ndim != 3 or frames.shape[1:] != (len(s), 3):
+            raise ValidationError(
+                f"frames must be [F, {len(s)}, 3]; got {tuple(frames.shape)}")
+        n_all = frames.shape[0]
+        if frame_weights is None:
+            w_all = np.ones(n_all)
+        else:
+            w_all = np.asarray(frame_weights, dtype=np.float64)
+            if len(w_all) != n_all:
+                raise ValidationError(
+                    f"number of weights ({len(w_all)}) does not match number of frames in "
+                    f"trajectory ({n_all})")
+            tot = float(np.sum(w_all))
+            if not np.isfinite(tot) or tot == 0.0 or abs(tot) < np.finfo(float).tiny:
+                raise ValidationError("sum of weights is zero or infinite")
+        if stride < 1:
+            raise ValidationError("stride must be >= 1")
+        sel = frames[::stride]
+        w = w_all[::stride]
+        wsum = float(np.sum(w))
+        if not np.isfinite(wsum) or wsum == 0.0 or abs(wsum) < np.finfo(float).tiny:
+            raise ValidationError(
+                f"weights of the {len(w)} averaged frames sum to {wsum}; cannot normalize")
+        req = make_request(s, self.formfactors, q, qmin, qmax, active, self.precision,
+                           frames=sel, frame_weights=w)
+        terms = solve(req, self.ctx)
+        if active is None:
+            return Intensity(q, terms[0].copy(), None)
+        return Intensity(q, combine(terms, active.excluded.effective_volume_scale(),
+                                    active.hydration.effective_contrast_density()), None)

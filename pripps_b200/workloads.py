@@ -1,0 +1,134 @@
+"""The five Debye workloads, built from seeded synthetic globules.
+
+  sphere_vacuum_1k     1,000 atoms, sphere R = 16 Å, vacuum, q ∈ [0, 0.5], nq = 500
+  sphere_solvent_10k   10,000 atoms, sphere R = 35 Å, FoXS Fraser excluded volume
+                       + Bernoulli(0.35) surface hydration, q ∈ [0, 0.5], nq = 500
+  ellipsoid_solvent_100k  100,000 atoms, prolate ellipsoid 80×40×40 Å, solvent as
+                       above, q ∈ [0, 1.0], nq = 1,000
+  trajectory_5k_256    256 frames of a 5,000-atom sphere (R = 25 Å), σ = 0.5 Å,
+                       Dirichlet(1) frame weights, vacuum, q ∈ [0, 0.5], nq = 300
+  stream               Poisson requests, N log-uniform 500–50,000 (sphere at the
+                       1k/16 Å density), nq 100–1000, qmax 0.3–1.0, 70 % solvent
+
+Form factors: the FoXS Cromer–Mann elements (data/foxs_elements.yaml), FoXS
+Fraser dummies ρ·V·exp(-V^{2/3} q²/16π) with ρ = 0.334 and the YAML displaced
+volumes (S: 4/3·π·1.68³), and the United H2O table for hydration.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+from functools import lru_cache
+from pathlib import Path
+from typing import Optional
+
+import numpy as np
+
+from . import synth
+from .debye import DebyeRequest
+from .formfactor import FormFactorMap, linear_q_values, read_formfactors
+from .solvent import (DEFAULT_BULK_DENSITY, ExcludedVolume, excluded_table, full_shell_weight,
+                      water_table)
+
+DATA = Path(__file__).resolve().parent / "data"
+
+
+@lru_cache(maxsize=1)
+def foxs() -> FormFactorMap:
+    return read_formfactors(DATA / "foxs_elements.yaml")
+
+
+def element_ids() -> np.ndarray:
+    m = foxs()
+    return np.array([m.id_of(e) for e in synth.ELEMENTS], dtype=np.int64)
+
+
+def tables(qv: np.ndarray, solvent: bool):
+    """Per-element (C, N, O, S) tables on the grid: F, C (FoXS Fraser) and
+    F_H2O; plus the fully-exposed shell weight of each element."""
+    m = foxs()
+    ids = element_ids()
+    ffA = m.table(ids, qv)
+    if not solvent:
+        return ffA, None, None, None
+    ffC = excluded_table(ExcludedVolume.fraser_foxs(1.0), m, ids, qv, DEFAULT_BULK_DENSITY)
+    ffW = water_table(m, qv)
+    wfull = np.array([full_shell_weight(m.kind(int(i)).radius, synth.PROBE) for i in ids])
+    return ffA, ffC, ffW, wfull
+
+
+def globule_request(g: synth.Globule, qmin: float, qmax: float, nq: int, solvent: bool,
+                    precision: str = "fp32", frames=None, frame_weights=None) -> DebyeRequest:
+    qv = linear_q_values(qmin, qmax, nq)
+    ffA, ffC, ffW, wfull = tables(qv, solvent)
+    hw = None
+    if solvent:
+        hw = np.where(g.exposed, wfull[g.elements], 0.0)
+    xyz = g.pos if frames is None else frames
+    return DebyeRequest(xyz, g.elements.astype(np.uint32), ffA, ffC, hw, ffW, qmin, qmax, nq,
+                        frame_weights, precision)
+
+
+@dataclass
+class Workload:
+    name: str
+    request: DebyeRequest
+    globule: synth.Globule
+
+    @property
+    def pairs(self) -> int:
+        n = self.request.n_atoms
+        return n * (n - 1) // 2
+
+    @property
+    def pair_q(self) -> int:
+        return self.pairs * self.request.nq * self.request.n_frames
+
+
+@lru_cache(maxsize=8)
+def _globule(n, axes, seed):
+    return synth.globule(n, axes, seed)
+
+
+def sphere_vacuum_1k(precision="fp64") -> Workload:
+    g = _globule(1000, (16.0, 16.0, 16.0), 0)
+    return Workload("sphere_vacuum_1k", globule_request(g, 0.0, 0.5, 500, False, precision), g)
+
+
+def sphere_solvent_10k(precision="fp32") -> Workload:
+    g = _globule(10_000, (35.0, 35.0, 35.0), 1)
+    return Workload("sphere_solvent_10k", globule_request(g, 0.0, 0.5, 500, True, precision), g)
+
+
+def ellipsoid_solvent_100k(precision="fp32") -> Workload:
+    g = _globule(100_000, (80.0, 40.0, 40.0), 2)
+    return Workload("ellipsoid_solvent_100k",
+                    globule_request(g, 0.0, 1.0, 1000, True, precision), g)
+
+
+def trajectory_5k_256(precision="fp32", n_frames: int = 256) -> Workload:
+    g = _globule(5000, (25.0, 25.0, 25.0), 3)
+    frames, w = synth.trajectory(g.pos, n_frames, 0.5, 3)
+    return Workload("trajectory_5k_256",
+                    globule_request(g, 0.0, 0.5, 300, False, precision, frames, w), g)
+
+
+def stream_request(sr: synth.StreamRequest, precision="fp32") -> Workload:
+    r = synth.sphere_radius_for(sr.n_atoms)
+    g = synth.globule(sr.n_atoms, (r, r, r), sr.seed)
+    return Workload(f"stream_{sr.n_atoms}",
+                    globule_request(g, 0.0, sr.qmax, sr.nq, sr.solvent, precision), g)
+
+
+def small_globule(n: int, seed: int, nq: int = 40, qmax: float = 0.5, solvent: bool = True,
+                  precision: str = "fp32", radius: Optional[float] = None) -> Workload:
+    r = radius if radius is not None else synth.sphere_radius_for(max(n, 8))
+    g = synth.globule(n, (r, r, r), seed)
+    return Workload(f"small_{n}", globule_request(g, 0.0, qmax, nq, solvent, precision), g)
+
+
+WORKLOADS = {
+    "sphere_vacuum_1k": sphere_vacuum_1k,
+    "sphere_solvent_10k": sphere_solvent_10k,
+    "ellipsoid_solvent_100k": ellipsoid_solvent_100k,
+    "trajectory_5k_256": trajectory_5k_256,
+}

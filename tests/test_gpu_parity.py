@@ -1,0 +1,286 @@
+"""Parity of the CUDA backend with the FP64 oracle, through the C ABI.
+
+Tolerances (stated by the target of this backend):
+  PD_FP64          every profile within 1e-10 of the oracle
+  PD_FP32_FP64RED  every profile within 1e-5 of the oracle
+Cross profiles (AC, AB, CB) change sign, so their error is normalised by
+sqrt(self_a·self_b) (see conftest.term_errors); self profiles are relative.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from conftest import load_golden, term_errors
+from oracle import oracle as O
+from pripps_b200 import _lib, workloads
+from pripps_b200.debye import DebyeRequest, solve
+
+pytestmark = pytest.mark.gpu
+
+TOL = {"fp64": 1e-10, "fp32": 1e-5}
+
+
+def _golden_request(g, precision, solvent):
+    return DebyeRequest(np.array(g["positions"]), np.array(g["species"]), np.array(g["ff_atoms"]),
+                        np.array(g["ff_excluded"]) if solvent else None,
+                        np.array(g["hyd_weights"]) if solvent else None,
+                        np.array(g["ff_water"]) if solvent else None,
+                        g["qmin"], g["qmax"], g["nq"], None, precision)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_pepsi_golden(gpu_ctx, precision):
+    g = load_golden("pepsi_4lzt.json")
+    req = _golden_request(g, precision, False)
+    t = solve(req, gpu_ctx)
+    oracle = np.array(g["oracle_vacuum"])
+    assert np.max(np.abs(t[0] - oracle) / oracle) < TOL[precision]
+    assert np.all(t[1:] == 0.0)
+    pepsi = np.array(g["pepsi_iat"])
+    assert np.max(np.abs(t[0] - pepsi) / pepsi) < g["pepsi_rel_tol"]
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_solvent_golden(gpu_ctx, precision):
+    g = load_golden("solvent_4lzt.json")
+    t = solve(_golden_request(g, precision, True), gpu_ctx)
+    err = term_errors(t, np.array(g["oracle_terms"]))
+    assert np.all(err < TOL[precision]), err
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_sphere_vacuum_1k_full(gpu_ctx, precision):
+    """1,000 atoms, nq = 500, the whole grid against the oracle."""
+    w = workloads.sphere_vacuum_1k(precision)
+    t = solve(w.request, gpu_ctx)
+    ref = O.terms_for_request(w.request)
+    err = term_errors(t, ref)
+    assert err[0] < TOL[precision], err
+    # I(0) = (Σf)² exactly up to FP64 rounding
+    f0 = w.request.ff_atoms[w.request.species, 0]
+    assert abs(t[0, 0] - f0.sum() ** 2) <= 1e-12 * f0.sum() ** 2
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_sphere_solvent_10k_q_subset(gpu_ctx, precision):
+    """10,000 atoms with solvent, nq = 500; oracle on a spread of grid points
+    (q = 0, the first steps, the middle and the end)."""
+    w = workloads.sphere_solvent_10k(precision)
+    t = solve(w.request, gpu_ctx)
+    qi = np.array([0, 1, 2, 7, 63, 64, 127, 128, 250, 383, 499])
+    ref = O.terms_for_request(w.request, q_index=qi)
+    err = term_errors(t[:, qi], ref)
+    assert np.all(err < TOL[precision]), err
+
+
+def _random_request(n, nq, solvent, weighted, seed, precision, qmin=0.0, qmax=0.6):
+    rng = np.random.default_rng(seed)
+    r = max(3.0, 2.0 * n ** (1 / 3))
+    xyz = rng.uniform(-r, r, (n, 3))
+    sp = rng.integers(0, 3, n)
+    ffA = rng.uniform(1, 8, (3, nq))
+    ffC = rng.uniform(0.2, 3, (3, nq)) if solvent else None
+    if solvent:
+        w = rng.uniform(0, 2, n) if weighted else np.where(rng.random(n) < 0.5, 1.25, 0.0)
+        fw = rng.uniform(5, 10, nq)
+    else:
+        w = fw = None
+    return DebyeRequest(xyz, sp, ffA, ffC, w, fw, qmin, qmax, nq, None, precision)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("n", [1, 2, 3, 33, 127, 129, 200])
+@pytest.mark.parametrize("nq", [1, 2, 37, 130])
+@pytest.mark.parametrize("mode", ["vacuum", "class", "weighted"])
+def test_edge_sizes(gpu_ctx, precision, n, nq, mode):
+    req = _random_request(n, nq, mode != "vacuum", mode == "weighted", 100 * n + nq, precision,
+                          qmin=0.05 if nq == 1 else 0.0)
+    t = solve(req, gpu_ctx)
+    ref = O.terms_for_request(req)
+    err = term_errors(t, ref)
+    assert np.all(err < TOL[precision]), (err, t[:, :3], ref[:, :3])
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_coincident_atoms(gpu_ctx, precision):
+    """Two dummies at the same point contribute sinc(0) = 1 at every q."""
+    xyz = np.array([[0, 0, 0], [0, 0, 0], [3.0, 0, 0]])
+    req = DebyeRequest(xyz, np.zeros(3), np.ones((1, 9)), None, None, None, 0.0, 0.8, 9, None,
+                       precision)
+    t = solve(req, gpu_ctx)
+    ref = O.terms_for_request(req)
+    assert np.max(np.abs(t[0] - ref[0]) / ref[0]) < TOL[precision]
+
+
+def test_fp32_vs_fp64_large_qr(gpu_ctx):
+    """Long pairs at high q (q·r up to ~230): FP32 recurrence against the
+    FP64 kernel on a 20,000-atom ellipsoid, q ∈ [0, 1.5], nq = 301."""
+    from pripps_b200 import synth
+    g = synth.globule(20_000, (80.0, 40.0, 40.0), 11)
+    r32 = workloads.globule_request(g, 0.0, 1.5, 301, True, "fp32")
+    r64 = workloads.globule_request(g, 0.0, 1.5, 301, True, "fp64")
+    t32, t64 = solve(r32, gpu_ctx), solve(r64, gpu_ctx)
+    err = term_errors(t32, t64)
+    assert np.all(err < 1e-5), err
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_deterministic(gpu_ctx, precision):
+    w = workloads.small_globule(3000, 5, nq=97, precision=precision)
+    a = solve(w.request, gpu_ctx)
+    b = solve(w.request, gpu_ctx)
+    assert np.array_equal(a, b)
+
+
+def test_cached_model_matches_one_shot(gpu_ctx):
+    """One kernel result feeds both paths, bit for bit
+    (src/lib.rs:535-566, :598-633)."""
+    from pripps_b200 import ExcludedVolume, Hydration, Pripps, SolventConfig, Structure
+    g = load_golden("solvent_4lzt.json")
+    from pripps_b200.formfactor import formfactors_from_yaml_str
+    pr = Pripps(workloads.foxs(), ctx=gpu_ctx)
+    glob = workloads.small_globule(500, 9).globule
+    ids = workloads.element_ids()[glob.elements]
+    s = Structure(glob.pos, ids)
+    weights = np.where(glob.exposed, 1.1, 0.0)
+    cfg = SolventConfig(ExcludedVolume.fraser_foxs(1.0), Hydration.sasa(0.03, weights=weights))
+    one = pr.intensity(s, 0.0, 0.3, 20, cfg)
+    model = pr.debye_model(s, 0.0, 0.3, 20, cfg)
+    cached = model.intensity(1.0, 0.03)
+    assert np.array_equal(one.total, cached.total)
+    assert one.contributions == cached.contributions
+    scaled = SolventConfig(ExcludedVolume.fraser_foxs(1.7))
+    one17 = pr.intensity(s, 0.0, 0.2, 8, scaled)
+    unit = pr.debye_model(s, 0.0, 0.2, 8, SolventConfig(ExcludedVolume.fraser_foxs(1.0)))
+    assert np.array_equal(one17.total, unit.intensity(1.7, 0.0).total)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_trajectory_batch(gpu_ctx, precision):
+    """All frames in one launch; the weighted mean against the oracle's
+    per-frame profiles combined in frame order (src/trajectory.rs:198-248)."""
+    from pripps_b200 import synth
+    g = synth.globule(400, (9.0, 9.0, 9.0), 21)
+    frames, wts = synth.trajectory(g.pos, 6, 0.5, 21)
+    req = workloads.globule_request(g, 0.0, 0.5, 31, True, precision, frames, wts)
+    t = solve(req, gpu_ctx)
+    acc = np.zeros((6, 31))
+    for f in range(6):
+        rf = workloads.globule_request(g, 0.0, 0.5, 31, True, precision, frames[f], None)
+        acc += wts[f] * O.terms_for_request(rf)
+    ref = acc / wts.sum()
+    err = term_errors(t, ref)
+    assert np.all(err < TOL[precision]), err
+
+
+def test_trajectory_stride_and_weights(gpu_ctx):
+    """One-hot weights select a frame; uniform weights give the mean; stride
+    renormalises by the consumed weight (src/lib.rs:1027-1099)."""
+    from pripps_b200 import Pripps, Structure, synth
+    pr = Pripps(workloads.foxs(), precision="fp64", ctx=gpu_ctx)
+    g = synth.globule(129, (8.0, 8.0, 8.0), 4)
+    s = Structure(g.pos, workloads.element_ids()[g.elements])
+    frames = np.stack([g.pos, 1.2 * g.pos])
+    run = lambda w, stride: pr.intensity(s, 0.05, 0.3, 8, frames=frames, frame_weights=w,
+                                         stride=stride).total
+    f0 = run([1.0, 0.0], 1)
+    f1 = run([0.0, 1.0], 1)
+    avg = run(None, 1)
+    s2 = run(None, 2)
+    close = lambda a, b: np.all(np.abs(a - b) <= 1e-9 * np.maximum(np.abs(a), 1.0))
+    assert not close(f0, f1)
+    assert close(avg, 0.5 * (f0 + f1))
+    assert close(s2, f0)
+
+
+def test_plan_execute_device_pointers(gpu_ctx):
+    """pd_plan_execute on device-resident coordinates gives the pd_solve
+    result bit for bit."""
+    import torch
+    w = workloads.small_globule(2500, 13, nq=150)
+    ref = solve(w.request, gpu_ctx)
+    lib = _lib.lib()
+    r = w.request.c_struct()
+    plan = C.c_void_p()
+    _lib.check(lib.pd_plan_create(gpu_ctx.handle, C.byref(r), C.byref(plan)), gpu_ctx.handle)
+    try:
+        xyz = torch.from_numpy(w.request.xyz).cuda()
+        out = torch.empty((6, w.request.nq), dtype=torch.float64, device="cuda")
+        stream = torch.cuda.current_stream().cuda_stream
+        for _ in range(2):
+            _lib.check(lib.pd_plan_execute(gpu_ctx.handle, plan, xyz.data_ptr(), out.data_ptr(),
+                                           stream), gpu_ctx.handle)
+        torch.cuda.synchronize()
+        assert np.array_equal(out.cpu().numpy(), ref)
+    finally:
+        lib.pd_plan_destroy(gpu_ctx.handle, plan)
+
+
+def test_serving_alone_equals_mixed(gpu_ctx):
+    """Requests submitted together run interleaved on the device; each result
+    equals its solo pd_solve bit for bit."""
+    from pripps_b200.serving import Server
+    reqs = [workloads.small_globule(n, s, nq=nq, solvent=sol).request
+            for n, s, nq, sol in [(3000, 1, 211, True), (700, 2, 97, False), (5000, 3, 150, True),
+                                  (1500, 4, 64, True), (9000, 5, 120, False), (40, 6, 33, True)]]
+    solo = [solve(r, gpu_ctx) for r in reqs]
+    srv = Server(gpu_ctx)
+    tickets = [srv.submit(r) for r in reqs]
+    outs = [srv.wait(t, timeout_s=120) for t in tickets]
+    for a, b in zip(outs, solo):
+        assert np.array_equal(a, b)
+    times = [srv.times(t) for t in tickets]
+    assert all(ts[0] <= ts[1] <= ts[2] for ts in times)
+
+
+def test_serving_budget_admission(gpu_ctx):
+    """With a budget that fits about one request, the loop admits them one at
+    a time and still completes all; a request that can never fit fails with
+    PD_EBUDGET."""
+    from pripps_b200.errors import DeviceError
+    from pripps_b200.serving import Server
+    reqs = [workloads.small_globule(4000, s, nq=200).request for s in range(3)]
+    ctx = _lib.Context(0, mem_budget_bytes=64 << 20)
+    try:
+        srv = Server(ctx)
+        solo = [solve(r, gpu_ctx) for r in reqs]
+        ts = [srv.submit(r) for r in reqs]
+        for t, ref in zip(ts, solo):
+            assert np.array_equal(srv.wait(t, timeout_s=120), ref)
+        big = workloads.small_globule(60_000, 1, nq=900).request
+        t = srv.submit(big)
+        with pytest.raises(DeviceError):
+            srv.wait(t, timeout_s=120)
+    finally:
+        ctx.close()
+
+
+def test_serving_cancel(gpu_ctx):
+    from pripps_b200.errors import DeviceError
+    from pripps_b200.serving import Server
+    srv = Server(gpu_ctx)
+    big = workloads.small_globule(30_000, 3, nq=600).request
+    t1 = srv.submit(big)
+    t2 = srv.submit(workloads.small_globule(500, 4, nq=40).request)
+    srv.cancel(t1)
+    with pytest.raises(DeviceError) as ei:
+        srv.wait(t1, timeout_s=120)
+    assert ei.value.code == _lib.PD_ECANCELED
+    out = srv.wait(t2, timeout_s=120)
+    assert out.shape == (6, 40)
+
+
+def test_autotune_and_fp32_probe(gpu_ctx):
+    lib = _lib.lib()
+    assert lib.pd_autotune(gpu_ctx.handle, 3000, 200, 0) == 0
+    k, tj = C.c_uint32(), C.c_uint32()
+    lib.pd_get_tuning(gpu_ctx.handle, 3000, 200, 0, C.byref(k), C.byref(tj))
+    assert k.value in (32, 64, 96, 128) and tj.value % 32 == 0
+    w = workloads.small_globule(3000, 7, nq=200)
+    t = solve(w.request, gpu_ctx)
+    ref = O.terms_for_request(w.request, q_index=np.array([0, 1, 50, 199]))
+    assert np.all(term_errors(t[:, [0, 1, 50, 199]], ref) < 1e-5)
+    a, b = C.c_double(), C.c_double()
+    assert lib.pd_measure_fp32_peak(gpu_ctx.handle, C.byref(a), C.byref(b)) == 0
+    assert 10.0 < a.value < 200.0
