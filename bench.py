@@ -202,9 +202,9 @@ def run_ours(args, ws, rank, local):
     r = req.c_struct()
     plan = C.c_void_p()
     _lib.check(lib.pd_plan_create(ctx.handle, C.byref(r), C.byref(plan)), ctx.handle)
-    kb, tj, ntile, dbytes, ubytes = (C.c_uint32(), C.c_uint32(), C.c_uint64(), C.c_uint64(),
-                                     C.c_uint64())
-    lib.pd_plan_info(plan, C.byref(kb), C.byref(tj), C.byref(ntile), C.byref(dbytes),
+    kb, tj, npt, ntile, dbytes, ubytes = (C.c_uint32(), C.c_uint32(), C.c_uint32(), C.c_uint64(),
+                                          C.c_uint64(), C.c_uint64())
+    lib.pd_plan_info(plan, C.byref(kb), C.byref(tj), C.byref(npt), C.byref(ntile), C.byref(dbytes),
                      C.byref(ubytes))
     xyz = torch.from_numpy(req.xyz).to(f"cuda:{local}")
     out = torch.empty((6, req.nq), dtype=torch.float64, device=f"cuda:{local}")
@@ -279,18 +279,18 @@ def run_ours(args, ws, rank, local):
     # ---- end to end through the C ABI with host buffers
     e2e_times = []
     res_host = None
-    for i in range(args.e2e_steps + 1):
+    for i in range(args.e2e_steps + 1 if args.e2e_steps > 0 else 0):
         t0 = time.perf_counter()
         res_host = solve(req, ctx)
         dt = time.perf_counter() - t0
         if i > 0:
             e2e_times.append(dt)
-    e2e_ms = 1e3 * sum(e2e_times) / len(e2e_times)
+    e2e_ms = 1e3 * sum(e2e_times) / len(e2e_times) if e2e_times else float("nan")
     if ws > 1:
         t = torch.tensor([e2e_ms], dtype=torch.float64, device=f"cuda:{local}")
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         e2e_ms = float(t.item())
-    same = bool(np.array_equal(res_host, result_dev))
+    same = bool(np.array_equal(res_host, result_dev)) if res_host is not None else None
     lib.pd_plan_destroy(ctx.handle, plan)
 
     if rank == 0:
@@ -329,8 +329,8 @@ def run_ours(args, ws, rank, local):
             "fp64_kernel": fp64,
             "cpu_baseline": cpu,
             "clocks": clk,
-            "tiles": {"q_block": kb.value, "j_chunk": tj.value, "tiles_per_solve": ntile.value,
-                      "device_bytes": dbytes.value},
+            "tiles": {"q_block": kb.value, "j_chunk": tj.value, "pairs_per_thread": npt.value,
+                      "tiles_per_solve": ntile.value, "device_bytes": dbytes.value},
         }
         print(json.dumps(line), flush=True)
     ctx.close()

@@ -131,10 +131,12 @@ int pd_plan_execute(pd_ctx *ctx, pd_plan *plan, const double *xyz_dev, double *o
 /* Blocking execution with HOST coordinates and a HOST [6][nq] result. */
 int pd_plan_execute_host(pd_ctx *ctx, pd_plan *plan, const double *xyz_host, double *out_terms);
 
-/* q-block length, atom-chunk length, tiles per execution, device bytes held
- * and bytes uploaded from the host when the plan is created. */
-int pd_plan_info(const pd_plan *plan, uint32_t *q_block, uint32_t *j_chunk, uint64_t *n_tiles,
-                 uint64_t *device_bytes, uint64_t *upload_bytes);
+/* q-block length, atom-chunk length, pairs per thread, tiles per execution,
+ * device bytes held and bytes uploaded from the host when the plan is
+ * created. */
+int pd_plan_info(const pd_plan *plan, uint32_t *q_block, uint32_t *j_chunk,
+                 uint32_t *pairs_per_thread, uint64_t *n_tiles, uint64_t *device_bytes,
+                 uint64_t *upload_bytes);
 
 /* Kernel timing: with profiling enabled every pd_plan_execute brackets its
  * pair kernel with CUDA events on the execution stream; pd_plan_pair_kernel_ms
@@ -172,14 +174,16 @@ int pd_combine(const double *terms, uint64_t nq, double volume_scale,
  * thread ("" if none); NULL ctx gives the last context-free failure. */
 const char *pd_last_error(pd_ctx *ctx);
 
-/* Kernel-shape choice for (n_atoms, nq, precision): the q-block length K of
- * the recurrence and the atom-chunk length of a tile, as picked by the
- * context's autotuner cache (pd_autotune fills it by timing candidates on the
- * device). Host-only for pd_get_tuning. */
+/* Kernel-shape choice for the (n_atoms, nq, precision) bucket (powers of two
+ * of n_atoms and nq): the q-block length K of the recurrence (FP32: 32, 64,
+ * 96, 128; FP64: 16, 32), the atom-chunk length of a tile (multiple of 32)
+ * and the pairs each thread advances together (FP32: 2 or 4). pd_autotune
+ * times the candidates on a synthetic globule of the bucket and stores the
+ * fastest; pd_get_tuning is host-only. */
 int pd_get_tuning(pd_ctx *ctx, uint64_t n_atoms, uint64_t nq, uint32_t precision,
-                  uint32_t *q_block, uint32_t *j_chunk);
+                  uint32_t *q_block, uint32_t *j_chunk, uint32_t *pairs_per_thread);
 int pd_set_tuning(pd_ctx *ctx, uint64_t n_atoms, uint64_t nq, uint32_t precision,
-                  uint32_t q_block, uint32_t j_chunk);
+                  uint32_t q_block, uint32_t j_chunk, uint32_t pairs_per_thread);
 int pd_autotune(pd_ctx *ctx, uint64_t n_atoms, uint64_t nq, uint32_t precision);
 
 /* Host-only planning report for a request (no device work): number of atom

@@ -56,6 +56,33 @@ static inline double dist3(const double *a, const double *b) {
     return sqrt(dx * dx + dy * dy + dz * dz);
 }
 
+/* Compensated variants: the same sums with the running accumulators in long
+ * double (64-bit mantissa on x86-64), used to tell the oracle's own rounding
+ * from a kernel's error when a comparison sits at the 1e-10 level. */
+static double self_intensity_ld(const double *xyz, const double *f, size_t n, double q) {
+    long double diagonal = 0.0L;
+    for (size_t i = 0; i < n; ++i) diagonal += (long double)f[i] * f[i];
+    if (n < 2) return (double)diagonal;
+    long double off = 0.0L;
+    for (size_t i = 0; i + 1 < n; ++i) {
+        const double *pi = xyz + 3 * i;
+        for (size_t j = i + 1; j < n; ++j) {
+            double r = dist3(pi, xyz + 3 * j);
+            off += (long double)(f[i] * f[j]) * pdo_sinc(q * r);
+        }
+    }
+    return (double)(2.0L * off + diagonal);
+}
+
+static double cross_intensity_ld(const double *axyz, const double *af, size_t na,
+                                 const double *bxyz, const double *bf, size_t nb, double q) {
+    long double total = 0.0L;
+    for (size_t a = 0; a < na; ++a)
+        for (size_t b = 0; b < nb; ++b)
+            total += (long double)(af[a] * bf[b]) * pdo_sinc(q * dist3(axyz + 3 * a, bxyz + 3 * b));
+    return (double)total;
+}
+
 /* src/debye.rs:214-232: diagonal Σf² first, then i<j (ascending j), then
  * 2.0.mul_add(off, diag). */
 double pdo_self_intensity(const double *xyz, const double *f, size_t n, double q) {
@@ -107,6 +134,7 @@ typedef struct {
     const uint32_t *q_index;
     size_t nqi;
     int solvent; /* 0: vacuum (out[t]), 1: six terms (out[6t..6t+5]) */
+    int precise; /* 1: long double accumulators */
     double *out;
     size_t next; /* shared work counter */
     pthread_mutex_t lock;
@@ -140,8 +168,13 @@ static void *pdo_worker(void *arg) {
             double q = jb->qv[k];
             /* formfactor_by_index (src/formfactor.rs:528-544) */
             for (size_t i = 0; i < n; ++i) fa[i] = jb->ff_atoms[(size_t)jb->species[i] * jb->nq + k];
+            double (*selfs)(const double *, const double *, size_t, double) =
+                jb->precise ? self_intensity_ld : pdo_self_intensity;
+            double (*cross)(const double *, const double *, size_t, const double *,
+                            const double *, size_t, double) =
+                jb->precise ? cross_intensity_ld : pdo_cross_intensity;
             if (!jb->solvent) {
-                jb->out[t] = pdo_self_intensity(jb->xyz, fa, n, q);
+                jb->out[t] = selfs(jb->xyz, fa, n, q);
                 continue;
             }
             /* DummySet::form_factors_at (src/solvent/mod.rs:357-374) */
@@ -152,12 +185,12 @@ static void *pdo_worker(void *arg) {
                 for (size_t i = 0; i < n_hyd; ++i) fb[i] = jb->hyd_weights[i] * shared;
             }
             double *o = jb->out + 6 * (size_t)t;
-            o[0] = pdo_self_intensity(jb->xyz, fa, n, q);
-            o[1] = pdo_self_intensity(jb->xyz, fc, n_exc, q);
-            o[2] = pdo_self_intensity(jb->xyz, fb, n_hyd, q);
-            o[3] = pdo_cross_intensity(jb->xyz, fa, n, jb->xyz, fc, n_exc, q);
-            o[4] = pdo_cross_intensity(jb->xyz, fa, n, jb->xyz, fb, n_hyd, q);
-            o[5] = pdo_cross_intensity(jb->xyz, fc, n_exc, jb->xyz, fb, n_hyd, q);
+            o[0] = selfs(jb->xyz, fa, n, q);
+            o[1] = selfs(jb->xyz, fc, n_exc, q);
+            o[2] = selfs(jb->xyz, fb, n_hyd, q);
+            o[3] = cross(jb->xyz, fa, n, jb->xyz, fc, n_exc, q);
+            o[4] = cross(jb->xyz, fa, n, jb->xyz, fb, n_hyd, q);
+            o[5] = cross(jb->xyz, fc, n_exc, jb->xyz, fb, n_hyd, q);
         }
     }
     free(fa);
@@ -202,13 +235,14 @@ static int pdo_run(pdo_job *jb, int n_threads) {
  * q_index selects which grid points to evaluate (NULL = all, n_q_index = nq);
  * out is [n_q_index][6] in the DebyeTerms field order
  * (atoms, excluded, hydration, atom_excluded, atom_hydration, excluded_hydration).
- * n_threads <= 0 uses every online core. Returns 0, or -1 on allocation failure.
+ * n_threads <= 0 uses every online core; precise != 0 accumulates in long
+ * double. Returns 0, or -1 on allocation failure.
  */
 int pdo_build_model(size_t n, const double *xyz, const uint32_t *species, size_t n_species,
                     const double *ff_atoms, const double *ff_excluded,
                     const double *hyd_weights, const double *ff_water, double qmin,
                     double qmax, size_t nq, const uint32_t *q_index, size_t n_q_index,
-                    int n_threads, double *out) {
+                    int n_threads, int precise, double *out) {
     (void)n_species;
     double *qv = (double *)malloc(sizeof(double) * (nq ? nq : 1));
     if (!qv) return -1;
@@ -226,6 +260,7 @@ int pdo_build_model(size_t n, const double *xyz, const uint32_t *species, size_t
     jb.q_index = q_index;
     jb.nqi = q_index ? n_q_index : nq;
     jb.solvent = 1;
+    jb.precise = precise;
     jb.out = out;
     int rc = pdo_run(&jb, n_threads);
     free(qv);
@@ -236,7 +271,7 @@ int pdo_build_model(size_t n, const double *xyz, const uint32_t *species, size_t
  * (src/debye.rs:58-60, :200-211). out is [n_q_index]. */
 int pdo_vacuum(size_t n, const double *xyz, const uint32_t *species, const double *ff_atoms,
                double qmin, double qmax, size_t nq, const uint32_t *q_index, size_t n_q_index,
-               int n_threads, double *out) {
+               int n_threads, int precise, double *out) {
     double *qv = (double *)malloc(sizeof(double) * (nq ? nq : 1));
     if (!qv) return -1;
     pdo_linear_q_values(qmin, qmax, nq, qv);
@@ -250,6 +285,7 @@ int pdo_vacuum(size_t n, const double *xyz, const uint32_t *species, const doubl
     jb.q_index = q_index;
     jb.nqi = q_index ? n_q_index : nq;
     jb.solvent = 0;
+    jb.precise = precise;
     jb.out = out;
     int rc = pdo_run(&jb, n_threads);
     free(qv);

@@ -47,10 +47,10 @@ def lib():
         L.pdo_build_model.restype = C.c_int
         L.pdo_build_model.argtypes = [C.c_size_t, _D, _U32, C.c_size_t, _D, _D, _D, _D,
                                       C.c_double, C.c_double, C.c_size_t, _U32, C.c_size_t,
-                                      C.c_int, _D]
+                                      C.c_int, C.c_int, _D]
         L.pdo_vacuum.restype = C.c_int
         L.pdo_vacuum.argtypes = [C.c_size_t, _D, _U32, _D, C.c_double, C.c_double, C.c_size_t,
-                                 _U32, C.c_size_t, C.c_int, _D]
+                                 _U32, C.c_size_t, C.c_int, C.c_int, _D]
         L.pdo_eval_gaussian.restype = C.c_double
         L.pdo_eval_gaussian.argtypes = [C.c_double, _D, _D, C.c_size_t, C.c_double]
         L.pdo_eval_polynomial.restype = C.c_double
@@ -94,8 +94,10 @@ def cross_intensity(axyz, af, bxyz, bf, q) -> float:
 
 
 def build_model(xyz, species, ff_atoms, ff_excluded=None, hyd_weights=None, ff_water=None,
-                qmin=0.0, qmax=0.5, nq=None, q_index=None, threads=0) -> np.ndarray:
-    """[len(q_index) or nq, 6] terms in DebyeTerms order (src/debye.rs:78-136)."""
+                qmin=0.0, qmax=0.5, nq=None, q_index=None, threads=0,
+                precise=False) -> np.ndarray:
+    """[len(q_index) or nq, 6] terms in DebyeTerms order (src/debye.rs:78-136).
+    precise=True: the same sums with long double accumulators."""
     xyz = _c(xyz).reshape(-1, 3)
     species = _c(species, np.uint32)
     ff_atoms = _c(ff_atoms)
@@ -107,14 +109,14 @@ def build_model(xyz, species, ff_atoms, ff_excluded=None, hyd_weights=None, ff_w
                                ff_atoms.shape[0], _d(ff_atoms), _d(_c(ff_excluded)),
                                _d(_c(hyd_weights)), _d(_c(ff_water)), qmin, qmax, nq,
                                None if qi is None else qi.ctypes.data_as(_U32), nqi, int(threads),
-                               _d(out))
+                               int(bool(precise)), _d(out))
     if rc != 0:
         raise MemoryError("oracle allocation failed")
     return out
 
 
 def vacuum(xyz, species, ff_atoms, qmin=0.0, qmax=0.5, nq=None, q_index=None,
-           threads=0) -> np.ndarray:
+           threads=0, precise=False) -> np.ndarray:
     xyz = _c(xyz).reshape(-1, 3)
     species = _c(species, np.uint32)
     ff_atoms = _c(ff_atoms)
@@ -124,7 +126,7 @@ def vacuum(xyz, species, ff_atoms, qmin=0.0, qmax=0.5, nq=None, q_index=None,
     out = np.empty(nqi)
     rc = lib().pdo_vacuum(len(species), _d(xyz), species.ctypes.data_as(_U32), _d(ff_atoms),
                           qmin, qmax, nq, None if qi is None else qi.ctypes.data_as(_U32), nqi,
-                          int(threads), _d(out))
+                          int(threads), int(bool(precise)), _d(out))
     if rc != 0:
         raise MemoryError("oracle allocation failed")
     return out
@@ -159,15 +161,15 @@ def sasa_full_weight(radius, probe) -> float:
     return lib().pdo_sasa_full_weight(float(radius), float(probe))
 
 
-def terms_for_request(req, q_index=None, threads=0) -> np.ndarray:
+def terms_for_request(req, q_index=None, threads=0, precise=False) -> np.ndarray:
     """Oracle terms [6, nq_sel] for a pripps_b200 DebyeRequest (one frame).
     Rows follow the C ABI order (DebyeTerms field order)."""
     if req.hyd_weights is None and req.ff_excluded is None:
         v = vacuum(req.xyz, req.species, req.ff_atoms, req.qmin, req.qmax, req.nq, q_index,
-                   threads)
+                   threads, precise)
         out = np.zeros((6, len(v)))
         out[0] = v
         return out
     t = build_model(req.xyz, req.species, req.ff_atoms, req.ff_excluded, req.hyd_weights,
-                    req.ff_water, req.qmin, req.qmax, req.nq, q_index, threads)
+                    req.ff_water, req.qmin, req.qmax, req.nq, q_index, threads, precise)
     return t.T.copy()

@@ -65,7 +65,7 @@ SIGNATURES = {
     "pd_plan_create": (C.c_int, [_P, C.POINTER(PdRequest), C.POINTER(_P)]),
     "pd_plan_execute": (C.c_int, [_P, _P, C.c_void_p, C.c_void_p, C.c_void_p]),
     "pd_plan_execute_host": (C.c_int, [_P, _P, _D, _D]),
-    "pd_plan_info": (C.c_int, [_P, _U32P, _U32P, _U64P, _U64P, _U64P]),
+    "pd_plan_info": (C.c_int, [_P, _U32P, _U32P, _U32P, _U64P, _U64P, _U64P]),
     "pd_plan_set_profiling": (C.c_int, [_P, _P, C.c_int]),
     "pd_plan_pair_kernel_ms": (C.c_int, [_P, _P, _D, _U64P]),
     "pd_plan_destroy": (None, [_P, _P]),
@@ -76,8 +76,9 @@ SIGNATURES = {
     "pd_ticket_times": (C.c_int, [_P, C.c_uint64, _D, _D, _D]),
     "pd_combine": (C.c_int, [_D, C.c_uint64, C.c_double, C.c_double, _D]),
     "pd_last_error": (C.c_char_p, [_P]),
-    "pd_get_tuning": (C.c_int, [_P, C.c_uint64, C.c_uint64, C.c_uint32, _U32P, _U32P]),
-    "pd_set_tuning": (C.c_int, [_P, C.c_uint64, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32]),
+    "pd_get_tuning": (C.c_int, [_P, C.c_uint64, C.c_uint64, C.c_uint32, _U32P, _U32P, _U32P]),
+    "pd_set_tuning": (C.c_int, [_P, C.c_uint64, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32,
+                                C.c_uint32]),
     "pd_autotune": (C.c_int, [_P, C.c_uint64, C.c_uint64, C.c_uint32]),
     "pd_plan_inspect": (C.c_int, [_P, C.POINTER(PdRequest), _U64P, _U64P, _U64P, _U64P]),
     "pd_measure_fp32_peak": (C.c_int, [_P, _D, _D]),

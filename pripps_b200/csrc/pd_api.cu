@@ -52,7 +52,7 @@ struct Layout {
     uint64_t upload_bytes;
     uint64_t hres;         // host-only: pinned landing area of the [6][nq] result
     uint64_t stage_bytes;  // pinned image size (upload + result area)
-    uint64_t centroid, atoms, slots, pairsum, terms, out, counter;
+    uint64_t centroid, radius, atoms, slots, pairsum, terms, out, counter;
     uint64_t total;
 };
 
@@ -85,6 +85,7 @@ Layout make_layout(const Plan &P, bool host_xyz) {
     L.hres = o;
     L.stage_bytes = align_up(o + 6 * nq * 8, 256);
     L.centroid = take(static_cast<uint64_t>(P.n_frames) * 3 * 8);
+    L.radius = take(static_cast<uint64_t>(P.n_frames) * 8);
     L.atoms = take(static_cast<uint64_t>(P.n_pad) * P.n_frames *
                    (P.precision == PD_FP64 ? sizeof(double4) : sizeof(float4)));
     L.slots = take(static_cast<uint64_t>(P.slots_per_frame) * P.n_frames * P.nv * P.tun.K * 8);
@@ -218,6 +219,7 @@ int stage_plan(pd_ctx *ctx, DevPlan &dp, const pd_request *req) {
     rd.gvalid = dp.dptr<int32_t>(L.gvalid);
     rd.qv = dp.dptr<double>(L.qv);
     rd.slots = dp.dptr<double>(L.slots);
+    rd.radius = dp.dptr<double>(L.radius);
     rd.qmin = P.qmin;
     rd.dq = P.dq;
     rd.n_pad = P.n_pad;
@@ -309,7 +311,9 @@ int finish_devplan(pd_ctx *ctx, DevPlan &dp, double *out_dev, cudaStream_t st) {
     PD_CUDA(ctx, pd::launch_reduce(dp.dptr<double>(L.slots), dp.dptr<int64_t>(L.lptr),
                                    dp.dptr<int64_t>(L.lidx), dp.dptr<PdPairDev>(L.pairs),
                                    dp.dptr<double>(L.qv), P.n_pairs, P.nq, P.tun.K, P.nv,
-                                   P.n_frames, P.slots_per_frame, dp.dptr<double>(L.pairsum), st));
+                                   P.n_frames, P.slots_per_frame, dp.dptr<double>(L.radius),
+                                   P.qmin, P.dq, P.precision == PD_FP32_FP64RED ? 1 : 0,
+                                   dp.dptr<double>(L.pairsum), st));
     PD_CUDA(ctx, pd::launch_combine(dp.dptr<double>(L.pairsum), dp.dptr<PdClassDev>(L.cls),
                                     dp.dptr<PdPairDev>(L.pairs), P.n_cls, P.n_pairs, P.nq, P.nv,
                                     P.n_frames, dp.dptr<double>(L.ffA),
@@ -334,7 +338,8 @@ int finish_devplan(pd_ctx *ctx, DevPlan &dp, double *out_dev, cudaStream_t st) {
 int pack_devplan(pd_ctx *ctx, DevPlan &dp, cudaStream_t st) {
     const Plan &P = dp.P;
     const Layout &L = dp.L;
-    PD_CUDA(ctx, pd::launch_centroid(dp.xyz_dev, P.n_atoms, P.n_frames, dp.dptr<double>(L.centroid), st));
+    PD_CUDA(ctx, pd::launch_centroid(dp.xyz_dev, P.n_atoms, P.n_frames, dp.dptr<double>(L.centroid),
+                                     dp.dptr<double>(L.radius), st));
     PD_CUDA(ctx, pd::launch_pack(dp.xyz_dev, P.has_hyd ? dp.dptr<double>(L.hw) : nullptr,
                                  dp.dptr<int32_t>(L.perm), dp.dptr<double>(L.centroid), P.n_atoms,
                                  P.n_pad, P.n_frames,
@@ -345,7 +350,8 @@ int pack_devplan(pd_ctx *ctx, DevPlan &dp, cudaStream_t st) {
 }
 
 int persistent_grid(pd_ctx *ctx, const Plan &P, int64_t n_jobs) {
-    const int per_sm = std::max(1, pd::pairs_blocks_per_sm(P.precision, P.tun.K, P.mode));
+    const int per_sm =
+        std::max(1, pd::pairs_blocks_per_sm(P.precision, P.tun.K, P.tun.NP, P.mode));
     const int64_t g = std::min<int64_t>(n_jobs, static_cast<int64_t>(ctx->sm_count) * per_sm);
     return static_cast<int>(std::max<int64_t>(g, 1));
 }
@@ -361,7 +367,7 @@ int run_devplan(pd_ctx *ctx, DevPlan &dp, double *out_dev, cudaStream_t st,
     if (ev) cudaEventRecord(ev->first, st);
     if (!P.jobs.empty()) {
         PD_CUDA(ctx, cudaMemsetAsync(dp.dptr<int>(L.counter), 0, sizeof(int), st));
-        PD_CUDA(ctx, pd::launch_pairs(P.precision, P.tun.K, P.mode, dp.dptr<PdJob>(L.jobs),
+        PD_CUDA(ctx, pd::launch_pairs(P.precision, P.tun.K, P.tun.NP, P.mode, dp.dptr<PdJob>(L.jobs),
                                       dp.dptr<int>(L.njobs), dp.dptr<PdReqDev>(L.req),
                                       dp.dptr<int>(L.counter),
                                       persistent_grid(ctx, P, static_cast<int64_t>(P.jobs.size())),
@@ -414,7 +420,7 @@ struct StepBuf {
     size_t cap_jobs = 0, cap_reqs = 0;
     cudaEvent_t ev = nullptr;
     bool busy = false;
-    std::map<std::tuple<int, int, int>, cudaGraphExec_t> graphs;  // (precision, K, mode)
+    std::map<std::tuple<int, int, int, int>, cudaGraphExec_t> graphs;  // (precision, K, NP, mode)
 };
 
 constexpr size_t STEP_MAX_JOBS = 1 << 14;
@@ -429,9 +435,9 @@ void ticket_fail(pd_ctx *ctx, const std::shared_ptr<PdTicket> &t, int code, cons
     if (t->dp.base || t->dp.stage) free_devplan(ctx, t->dp, st);
 }
 
-int step_graph(pd_ctx *ctx, StepBuf &sb, int precision, int K, int mode, cudaStream_t st,
-               cudaGraphExec_t *out) {
-    auto key = std::make_tuple(precision, K, mode);
+int step_graph(pd_ctx *ctx, StepBuf &sb, int precision, int K, int NP, int mode,
+               cudaStream_t st, cudaGraphExec_t *out) {
+    auto key = std::make_tuple(precision, K, NP, mode);
     auto it = sb.graphs.find(key);
     if (it != sb.graphs.end()) {
         *out = it->second;
@@ -440,6 +446,7 @@ int step_graph(pd_ctx *ctx, StepBuf &sb, int precision, int K, int mode, cudaStr
     Plan dummy;
     dummy.precision = precision;
     dummy.tun.K = K;
+    dummy.tun.NP = NP;
     dummy.mode = mode;
     const int grid = persistent_grid(ctx, dummy, 1 << 30);
     cudaGraph_t g = nullptr;
@@ -448,7 +455,7 @@ int step_graph(pd_ctx *ctx, StepBuf &sb, int precision, int K, int mode, cudaStr
     cudaMemcpyAsync(sb.d_reqs, sb.h_reqs, sb.cap_reqs * sizeof(PdReqDev), cudaMemcpyHostToDevice, st);
     cudaMemcpyAsync(sb.d_jobs, sb.h_jobs, sb.cap_jobs * sizeof(PdJob), cudaMemcpyHostToDevice, st);
     cudaMemsetAsync(sb.d_counter, 0, sizeof(int), st);
-    pd::launch_pairs(precision, K, mode, sb.d_jobs, sb.d_n, sb.d_reqs, sb.d_counter, grid, st);
+    pd::launch_pairs(precision, K, NP, mode, sb.d_jobs, sb.d_n, sb.d_reqs, sb.d_counter, grid, st);
     PD_CUDA(ctx, cudaStreamEndCapture(st, &g));
     cudaGraphExec_t ge = nullptr;
     cudaError_t e = cudaGraphInstantiate(&ge, g, 0);
@@ -566,10 +573,12 @@ void worker_main(pd_ctx *ctx) {
         std::vector<std::shared_ptr<PdTicket>> finished_now;
         if (head) {
             const int prec = head->dp.P.precision, K = head->dp.P.tun.K, mode = head->dp.P.mode;
+            const int NP = head->dp.P.tun.NP;
             std::vector<std::shared_ptr<PdTicket>> members;
             for (auto &t : active)
                 if (!t->canceled && t->next_job < t->dp.P.jobs.size() &&
                     t->dp.P.precision == prec && t->dp.P.tun.K == K && t->dp.P.mode == mode &&
+                    t->dp.P.tun.NP == NP &&
                     members.size() < STEP_MAX_REQS)
                     members.push_back(t);
             size_t nj = 0;
@@ -600,7 +609,7 @@ void worker_main(pd_ctx *ctx) {
             }
             *sb.h_n = static_cast<int>(nj);
             cudaGraphExec_t ge = nullptr;
-            int rc = step_graph(ctx, sb, prec, K, mode, st, &ge);
+            int rc = step_graph(ctx, sb, prec, K, NP, mode, st, &ge);
             if (rc == PD_OK && cudaGraphLaunch(ge, st) == cudaSuccess) {
                 ctx->launches += 1;
             } else {
@@ -931,9 +940,10 @@ void pd_plan_destroy(pd_ctx *ctx, pd_plan *plan) {
     delete plan;
 }
 
-int pd_plan_info(const pd_plan *plan, uint32_t *q_block, uint32_t *j_chunk, uint64_t *n_tiles,
-                 uint64_t *device_bytes, uint64_t *upload_bytes) {
+int pd_plan_info(const pd_plan *plan, uint32_t *q_block, uint32_t *j_chunk, uint32_t *pairs_per_thread,
+                 uint64_t *n_tiles, uint64_t *device_bytes, uint64_t *upload_bytes) {
     if (!plan) return PD_EINVAL;
+    if (pairs_per_thread) *pairs_per_thread = static_cast<uint32_t>(plan->dp.P.tun.NP);
     if (upload_bytes) *upload_bytes = plan->dp.L.upload_bytes;
     if (q_block) *q_block = static_cast<uint32_t>(plan->dp.P.tun.K);
     if (j_chunk) *j_chunk = static_cast<uint32_t>(plan->dp.P.tun.TJ);
@@ -1064,19 +1074,23 @@ int pd_combine(const double *terms, uint64_t nq, double vs, double c, double *to
 }
 
 int pd_get_tuning(pd_ctx *ctx, uint64_t n_atoms, uint64_t nq, uint32_t precision,
-                  uint32_t *q_block, uint32_t *j_chunk) {
+                  uint32_t *q_block, uint32_t *j_chunk, uint32_t *pairs_per_thread) {
     Tuning t = tuning_for(ctx, static_cast<int64_t>(n_atoms), static_cast<int64_t>(nq),
                           static_cast<int>(precision));
     if (q_block) *q_block = static_cast<uint32_t>(t.K);
     if (j_chunk) *j_chunk = static_cast<uint32_t>(t.TJ);
+    if (pairs_per_thread) *pairs_per_thread = static_cast<uint32_t>(t.NP);
     return PD_OK;
 }
 
 int pd_set_tuning(pd_ctx *ctx, uint64_t n_atoms, uint64_t nq, uint32_t precision, uint32_t q_block,
-                  uint32_t j_chunk) {
+                  uint32_t j_chunk, uint32_t pairs_per_thread) {
     if (!ctx) return PD_EINVAL;
+    const int np = precision == PD_FP64 ? 1 : static_cast<int>(pairs_per_thread);
     if (!pd::valid_q_block(static_cast<int>(precision), static_cast<int>(q_block)) ||
-        j_chunk < 32 || j_chunk % 32 != 0) {
+        j_chunk < 32 || j_chunk % 32 != 0 ||
+        (precision != PD_FP64 &&
+         !pd::valid_shape(static_cast<int>(precision), PD_MODE_CLASS, static_cast<int>(q_block), np))) {
         ctx->set_error("invalid tuning");
         return PD_EINVAL;
     }
@@ -1086,6 +1100,7 @@ int pd_set_tuning(pd_ctx *ctx, uint64_t n_atoms, uint64_t nq, uint32_t precision
     Tuning t;
     t.K = static_cast<int>(q_block);
     t.TJ = static_cast<int>(j_chunk);
+    t.NP = np;
     ctx->tuning[std::make_tuple(static_cast<int>(precision), nb, qb)] = t;
     return PD_OK;
 }
@@ -1122,8 +1137,10 @@ int pd_autotune(pd_ctx *ctx, uint64_t n_atoms, uint64_t nq, uint32_t precision) 
     rq.qmin = 0.0;
     rq.qmax = 0.5;
     rq.nq = nq;
-    std::vector<int> Ks = precision == PD_FP64 ? std::vector<int>{16, 32}
-                                               : std::vector<int>{32, 64, 96, 128};
+    std::vector<std::pair<int, int>> shapes =
+        precision == PD_FP64
+            ? std::vector<std::pair<int, int>>{{16, 1}, {32, 1}}
+            : std::vector<std::pair<int, int>>{{32, 4}, {64, 2}, {64, 4}, {96, 2}, {128, 2}, {128, 4}};
     std::vector<int> TJs = {512, 1024, 2048, 4096, 8192};
     double best = 1e300;
     Tuning best_t = pd::default_tuning(static_cast<int64_t>(n_atoms), static_cast<int64_t>(nq),
@@ -1136,11 +1153,12 @@ int pd_autotune(pd_ctx *ctx, uint64_t n_atoms, uint64_t nq, uint32_t precision) 
     cudaMalloc(reinterpret_cast<void **>(&xyz_dev), xyz.size() * 8);
     cudaMalloc(reinterpret_cast<void **>(&out_dev), 6 * nq * 8);
     cudaMemcpy(xyz_dev, xyz.data(), xyz.size() * 8, cudaMemcpyHostToDevice);
-    for (int K : Ks) {
+    for (auto shape : shapes) {
+        const int K = shape.first, NP = shape.second;
         if (precision != PD_FP64 && nq <= 32 && K != 32) continue;
         for (int TJ : TJs) {
             if (TJ > static_cast<int>(2 * n_atoms) && TJ != TJs.front()) continue;
-            pd_set_tuning(ctx, n_atoms, nq, precision, K, TJ);
+            pd_set_tuning(ctx, n_atoms, nq, precision, K, TJ, NP);
             pd_plan *plan = nullptr;
             if (pd_plan_create(ctx, &rq, &plan) != PD_OK) continue;
             float ms = 0;
@@ -1156,6 +1174,7 @@ int pd_autotune(pd_ctx *ctx, uint64_t n_atoms, uint64_t nq, uint32_t precision) 
                 best = ms;
                 best_t.K = K;
                 best_t.TJ = TJ;
+                best_t.NP = NP;
             }
         }
     }
@@ -1163,7 +1182,7 @@ int pd_autotune(pd_ctx *ctx, uint64_t n_atoms, uint64_t nq, uint32_t precision) 
     cudaFree(out_dev);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    return pd_set_tuning(ctx, n_atoms, nq, precision, best_t.K, best_t.TJ);
+    return pd_set_tuning(ctx, n_atoms, nq, precision, best_t.K, best_t.TJ, best_t.NP);
 }
 
 int pd_plan_inspect(pd_ctx *ctx, const pd_request *req, uint64_t *n_classes, uint64_t *n_padded,

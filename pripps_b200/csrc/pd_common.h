@@ -56,6 +56,7 @@ struct PdReqDev {
     const int32_t *gvalid;    // [n_pad / 32] valid atoms per granule
     const double *qv;         // [nq] grid (FP64 form reads it directly)
     double *slots;            // [n_slots][nv][K]
+    const double *radius;     // [n_frames] largest atom distance from the centroid
     double qmin, dq;          // grid origin and step
     int32_t n_pad;
     int32_t nq;

@@ -59,15 +59,30 @@ __device__ __forceinline__ float cos_small(float h) {
     return fmaf(h2, p, 1.0f);
 }
 
+// sin and cos of an FP32 angle |th| <~ 1e4 without a branch: th = n·π/2 + t
+// with a two-part π/2 (1.5703125 is exact in 8 bits, so n·1.5703125 is exact
+// for n < 2^15), then the Taylor forms on |t| <= π/4 and the quadrant of n.
+__device__ __forceinline__ void sincos_reduced(float th, float &s, float &c) {
+    const float n = rintf(th * 0.636619772f);
+    float t = fmaf(-n, 1.5703125f, th);
+    t = fmaf(-n, 4.83826794897e-4f, t);
+    const float st = sin_small(t), ct = cos_small(t);
+    const int qd = static_cast<int>(n);
+    const bool swap = (qd & 1) != 0;
+    float ss = swap ? ct : st;
+    float cc = swap ? st : ct;
+    s = (qd & 2) ? -ss : ss;
+    c = ((qd + 1) & 2) ? -cc : cc;
+}
+
 // Seed of one pair for a q-block: the recurrence state (u, d), the negated
 // step coefficient -α and the weights for even and odd steps (σ^k folded in).
 struct PairSeed {
     float u, d, na, we, wo;
 };
 
-__device__ __forceinline__ PairSeed pair_seed(float4 pi, float4 pj, float scale_if_valid,
-                                              bool valid, float qs_hi, float qs_lo,
-                                              float dq_hi, float dq_lo) {
+__device__ __forceinline__ PairSeed pair_seed(float4 pi, float4 pj, bool valid, float qs_hi,
+                                              float qs_lo, float dq_hi, float dq_lo) {
     const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
     float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
     // Coincident points: sinc(0) = 1, i.e. sin(q r)/r -> q; r = 1e-6 Å gives
@@ -86,19 +101,92 @@ __device__ __forceinline__ PairSeed pair_seed(float4 pi, float4 pj, float scale_
     const float h = 0.5f * xr;
     const float sh = sin_small(h), ch = cos_small(h);
     float s0, c0;
-    sincosf(th, &s0, &c0);
+    sincos_reduced(th, s0, c0);
     PairSeed ps;
-    ps.u = s0;                                       // u_0 = sin θ
-    ps.d = 2.0f * sh * fmaf(c0, ch, s0 * sh);        // u_0 − u_{−1} = 2 sin h cos(θ − h)
-    ps.na = -4.0f * sh * sh;                         // −α
-    const float w = valid ? scale_if_valid * inv_r : 0.0f;
+    ps.u = s0;                                 // u_0 = sin θ
+    ps.d = 2.0f * sh * fmaf(c0, ch, s0 * sh);  // u_0 − u_{−1} = 2 sin h cos(θ − h)
+    ps.na = -4.0f * sh * sh;                   // −α
+    const float w = valid ? inv_r : 0.0f;
     ps.we = w;
     ps.wo = sgn * w;
     return ps;
 }
 
+// A q-block uses the residual form when q_s·(2·radius) < 4: there the terms
+// sin(q r)/r are all close to q, and accumulating them directly in FP32 would
+// round with a systematic bias; the kernel accumulates sin(q r)/r − q instead
+// and the reduction adds (pair count)·q back in FP64. Both kernels evaluate
+// this predicate from the same FP64 inputs.
+__host__ __device__ __forceinline__ bool residual_block(int qb, int K, double qmin, double dq,
+                                                        double radius) {
+    const double qs = qmin + static_cast<double>(qb) * K * dq;
+    return qs * (2.0 * radius) < 4.0;
+}
+
 // ---------------------------------------------------------------- K1 (FP32)
-template <int K, int MODE>
+// NP pairs per thread per pass: independent recurrence chains for ILP.
+template <int K, int MODE, int NP, bool RESID>
+__device__ __forceinline__ void pairs_range(const float4 *__restrict__ at, float4 pi, int i,
+                                            bool ivalid, int j0, int j1, float qs_hi,
+                                            float qs_lo, float dq_hi, float dq_lo,
+                                            float (&acc)[(MODE == PD_MODE_WEIGHTED) ? 2 : 1][K]) {
+    constexpr int NACC = (MODE == PD_MODE_WEIGHTED) ? 2 : 1;
+    for (int j = j0; j < j1; j += NP) {
+        PairSeed S[NP];
+        float wj[NP];
+        float vsum = 0.0f, vwsum = 0.0f;
+#pragma unroll
+        for (int p = 0; p < NP; ++p) {
+            const int jj = j + p;
+            const bool inr = jj < j1;
+            const float4 pj = __ldg(at + (inr ? jj : j));
+            const bool valid = ivalid && inr && (jj > i);
+            S[p] = pair_seed(pi, pj, valid, qs_hi, qs_lo, dq_hi, dq_lo);
+            wj[p] = pj.w;
+            if (RESID) {
+                vsum += valid ? 1.0f : 0.0f;
+                if (MODE == PD_MODE_WEIGHTED) vwsum += valid ? pj.w : 0.0f;
+            }
+        }
+        // q_k = q_s + k·Δq is the same in every pass of this loop; passing q_s
+        // through an opaque move keeps the compiler from hoisting all K values
+        // into registers.
+        float qs_pass = qs_hi;
+        if (RESID) asm volatile("mov.b32 %0, %0;" : "+f"(qs_pass));
+        float we_w[NP], wo_w[NP];
+        if (MODE == PD_MODE_WEIGHTED) {
+#pragma unroll
+            for (int p = 0; p < NP; ++p) {
+                we_w[p] = S[p].we * wj[p];
+                wo_w[p] = S[p].wo * wj[p];
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < K; k += 2) {
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                if (RESID) {
+                    const float qk = fmaf(static_cast<float>(k + h), dq_hi, qs_pass);
+                    acc[0][k + h] = fmaf(-vsum, qk, acc[0][k + h]);
+                    if (MODE == PD_MODE_WEIGHTED)
+                        acc[NACC - 1][k + h] = fmaf(-vwsum, qk, acc[NACC - 1][k + h]);
+                }
+#pragma unroll
+                for (int p = 0; p < NP; ++p) {
+                    const float w = h ? S[p].wo : S[p].we;
+                    acc[0][k + h] = fmaf(w, S[p].u, acc[0][k + h]);
+                    if (MODE == PD_MODE_WEIGHTED)
+                        acc[NACC - 1][k + h] =
+                            fmaf(h ? wo_w[p] : we_w[p], S[p].u, acc[NACC - 1][k + h]);
+                    S[p].d = fmaf(S[p].na, S[p].u, S[p].d);
+                    S[p].u += S[p].d;
+                }
+            }
+        }
+    }
+}
+
+template <int K, int MODE, int NP>
 __global__ void __launch_bounds__(PD_THREADS) pd_pairs_fp32(const PdJob *__restrict__ jobs,
                                                             const int *__restrict__ n_jobs_ptr,
                                                             const PdReqDev *__restrict__ reqs,
@@ -133,54 +221,12 @@ __global__ void __launch_bounds__(PD_THREADS) pd_pairs_fp32(const PdJob *__restr
 #pragma unroll
             for (int k = 0; k < K; ++k) acc[a][k] = 0.0f;
 
-        for (int j = jb.j0; j < jb.j1; j += 2) {
-            const bool has_b = (j + 1) < jb.j1;
-            const float4 pa = __ldg(at + j);
-            const float4 pb = __ldg(at + (has_b ? j + 1 : j));
-            PairSeed A = pair_seed(pi, pa, 1.0f, ivalid && (j > i), qs_hi, qs_lo, dq_hi, dq_lo);
-            PairSeed B = pair_seed(pi, pb, 1.0f, ivalid && has_b && (j + 1 > i), qs_hi, qs_lo,
-                                   dq_hi, dq_lo);
-            if (MODE == PD_MODE_CLASS) {
-#pragma unroll
-                for (int k = 0; k < K; k += 2) {
-                    acc[0][k] = fmaf(A.we, A.u, acc[0][k]);
-                    A.d = fmaf(A.na, A.u, A.d);
-                    A.u += A.d;
-                    acc[0][k] = fmaf(B.we, B.u, acc[0][k]);
-                    B.d = fmaf(B.na, B.u, B.d);
-                    B.u += B.d;
-                    acc[0][k + 1] = fmaf(A.wo, A.u, acc[0][k + 1]);
-                    A.d = fmaf(A.na, A.u, A.d);
-                    A.u += A.d;
-                    acc[0][k + 1] = fmaf(B.wo, B.u, acc[0][k + 1]);
-                    B.d = fmaf(B.na, B.u, B.d);
-                    B.u += B.d;
-                }
-            } else {
-                const float wa = pa.w, wb = pb.w;
-                const float awe = A.we * wa, awo = A.wo * wa;
-                const float bwe = B.we * wb, bwo = B.wo * wb;
-#pragma unroll
-                for (int k = 0; k < K; k += 2) {
-                    acc[0][k] = fmaf(A.we, A.u, acc[0][k]);
-                    acc[NACC - 1][k] = fmaf(awe, A.u, acc[NACC - 1][k]);
-                    A.d = fmaf(A.na, A.u, A.d);
-                    A.u += A.d;
-                    acc[0][k] = fmaf(B.we, B.u, acc[0][k]);
-                    acc[NACC - 1][k] = fmaf(bwe, B.u, acc[NACC - 1][k]);
-                    B.d = fmaf(B.na, B.u, B.d);
-                    B.u += B.d;
-                    acc[0][k + 1] = fmaf(A.wo, A.u, acc[0][k + 1]);
-                    acc[NACC - 1][k + 1] = fmaf(awo, A.u, acc[NACC - 1][k + 1]);
-                    A.d = fmaf(A.na, A.u, A.d);
-                    A.u += A.d;
-                    acc[0][k + 1] = fmaf(B.wo, B.u, acc[0][k + 1]);
-                    acc[NACC - 1][k + 1] = fmaf(bwo, B.u, acc[NACC - 1][k + 1]);
-                    B.d = fmaf(B.na, B.u, B.d);
-                    B.u += B.d;
-                }
-            }
-        }
+        if (residual_block(jb.qb, K, rq.qmin, rq.dq, rq.radius[jb.frame]))
+            pairs_range<K, MODE, NP, true>(at, pi, i, ivalid, jb.j0, jb.j1, qs_hi, qs_lo, dq_hi,
+                                           dq_lo, acc);
+        else
+            pairs_range<K, MODE, NP, false>(at, pi, i, ivalid, jb.j0, jb.j1, qs_hi, qs_lo, dq_hi,
+                                            dq_lo, acc);
 
         // Warp-reduce and write this warp's slot: [nv][K] FP64 values.
         double *slot = rq.slots + (jb.slot + warp) * static_cast<int64_t>(K) *
@@ -286,9 +332,10 @@ __global__ void __launch_bounds__(PD_THREADS) pd_pairs_fp64(const PdJob *__restr
 }
 
 // ------------------------------------------------------- pack and centroid
-// Per-frame centroid of the input positions (FP64, fixed-order tree).
+// Per-frame centroid of the input positions (FP64, fixed-order tree) and the
+// largest distance of an atom from it.
 __global__ void pd_centroid(const double *__restrict__ xyz, int64_t n_atoms,
-                            double *__restrict__ centroid) {
+                            double *__restrict__ centroid, double *__restrict__ radius) {
     __shared__ double red[3][256];
     const int f = blockIdx.x;
     const double *p = xyz + static_cast<size_t>(f) * n_atoms * 3;
@@ -310,11 +357,27 @@ __global__ void pd_centroid(const double *__restrict__ xyz, int64_t n_atoms,
         }
         __syncthreads();
     }
+    const double cx = red[0][0] / static_cast<double>(n_atoms);
+    const double cy = red[1][0] / static_cast<double>(n_atoms);
+    const double cz = red[2][0] / static_cast<double>(n_atoms);
+    __syncthreads();
     if (threadIdx.x == 0) {
-        centroid[3 * f] = red[0][0] / static_cast<double>(n_atoms);
-        centroid[3 * f + 1] = red[1][0] / static_cast<double>(n_atoms);
-        centroid[3 * f + 2] = red[2][0] / static_cast<double>(n_atoms);
+        centroid[3 * f] = cx;
+        centroid[3 * f + 1] = cy;
+        centroid[3 * f + 2] = cz;
     }
+    double rm = 0.0;
+    for (int64_t i = threadIdx.x; i < n_atoms; i += blockDim.x) {
+        const double dx = p[3 * i] - cx, dy = p[3 * i + 1] - cy, dz = p[3 * i + 2] - cz;
+        rm = fmax(rm, dx * dx + dy * dy + dz * dz);
+    }
+    red[0][threadIdx.x] = rm;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) red[0][threadIdx.x] = fmax(red[0][threadIdx.x], red[0][threadIdx.x + s]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) radius[f] = sqrt(red[0][0]);
 }
 
 // Gather positions into the class-sorted, padded layout, centred per frame.
@@ -348,7 +411,8 @@ __global__ void pd_reduce_pairs(const double *__restrict__ slots, const int64_t 
                                 const int64_t *__restrict__ lidx, const PdPairDev *__restrict__ pairs,
                                 const double *__restrict__ qv, int32_t n_pairs, int32_t nq,
                                 int32_t K, int32_t nv, int32_t n_frames, int64_t slots_per_frame,
-                                double *__restrict__ pairsum) {
+                                const double *__restrict__ radius, double qmin, double dq,
+                                int32_t residual_form, double *__restrict__ pairsum) {
     const int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
     const int64_t per_frame = static_cast<int64_t>(n_pairs) * nq;
     if (t >= per_frame * n_frames) return;
@@ -368,6 +432,8 @@ __global__ void pd_reduce_pairs(const double *__restrict__ slots, const int64_t 
             for (int v = 0; v < nv; ++v) s[v] += sl[v * K + kk];
         }
         for (int v = 0; v < nv; ++v) s[v] /= qval;
+        if (residual_form && residual_block(qb, K, qmin, dq, radius[f]))
+            for (int v = 0; v < nv; ++v) s[v] += pairs[p].q0[v];
     } else {
         for (int v = 0; v < 4; ++v) s[v] = pairs[p].q0[v];
     }
@@ -507,10 +573,10 @@ __global__ void pd_ffma2_probe(float *out, int iters, float a, float b) {
 }
 
 // ------------------------------------------------------------ launchers
-template <int K, int MODE>
+template <int K, int MODE, int NP>
 static cudaError_t launch_fp32_t(const PdJob *jobs, const int *n_jobs, const PdReqDev *reqs,
                                  int *counter, int grid, cudaStream_t st) {
-    pd_pairs_fp32<K, MODE><<<grid, PD_THREADS, 0, st>>>(jobs, n_jobs, reqs, counter);
+    pd_pairs_fp32<K, MODE, NP><<<grid, PD_THREADS, 0, st>>>(jobs, n_jobs, reqs, counter);
     return cudaGetLastError();
 }
 template <int K, int MODE>
@@ -519,11 +585,10 @@ static cudaError_t launch_fp64_t(const PdJob *jobs, const int *n_jobs, const PdR
     pd_pairs_fp64<K, MODE><<<grid, PD_THREADS, 0, st>>>(jobs, n_jobs, reqs, counter);
     return cudaGetLastError();
 }
-
-template <int K, int MODE>
+template <int K, int MODE, int NP>
 static int occupancy_fp32() {
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, pd_pairs_fp32<K, MODE>, PD_THREADS, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, pd_pairs_fp32<K, MODE, NP>, PD_THREADS, 0);
     return n;
 }
 template <int K, int MODE>
@@ -533,63 +598,56 @@ static int occupancy_fp64() {
     return n;
 }
 
+// (K, NP) shapes instantiated for the FP32 form; the weighted mode (two
+// accumulators per q) only up to K = 64 to stay within 255 registers.
+bool valid_shape(int precision, int mode, int K, int NP) {
+    if (precision == 1) return (K == 16 || K == 32) && NP == 1;
+    if (mode == PD_MODE_WEIGHTED) return (K == 32 && NP == 2) || (K == 64 && NP == 2);
+    return (K == 32 && NP == 4) || (K == 64 && (NP == 2 || NP == 4)) || (K == 96 && NP == 2) ||
+           (K == 128 && (NP == 2 || NP == 4));
+}
+
 bool valid_q_block(int precision, int K) {
     if (precision == 1) return K == 16 || K == 32;
     return K == 32 || K == 64 || K == 96 || K == 128;
 }
 
-#define PD_DISPATCH_FP32(K)                                                                  \
-    case K:                                                                                  \
-        return mode == PD_MODE_CLASS ? launch_fp32_t<K, PD_MODE_CLASS>(jobs, n_jobs, reqs,  \
-                                                                         counter, grid, st) \
-                                     : launch_fp32_t<K, PD_MODE_WEIGHTED>(jobs, n_jobs, reqs, \
-                                                                          counter, grid, st);
-#define PD_DISPATCH_FP64(K)                                                                  \
-    case K:                                                                                  \
-        return mode == PD_MODE_CLASS ? launch_fp64_t<K, PD_MODE_CLASS>(jobs, n_jobs, reqs,  \
-                                                                         counter, grid, st) \
-                                     : launch_fp64_t<K, PD_MODE_WEIGHTED>(jobs, n_jobs, reqs, \
-                                                                          counter, grid, st);
+#define PD_F32(K, M, NP)                                                                 \
+    if (K_ == K && mode == M && NP_ == NP)                                               \
+        return launch_fp32_t<K, M, NP>(jobs, n_jobs, reqs, counter, grid, st);
+#define PD_F64(K, M) \
+    if (K_ == K && mode == M) return launch_fp64_t<K, M>(jobs, n_jobs, reqs, counter, grid, st);
 
-cudaError_t launch_pairs(int precision, int K, int mode, const PdJob *jobs, const int *n_jobs,
-                         const PdReqDev *reqs, int *counter, int grid, cudaStream_t st) {
+cudaError_t launch_pairs(int precision, int K_, int NP_, int mode, const PdJob *jobs,
+                         const int *n_jobs, const PdReqDev *reqs, int *counter, int grid,
+                         cudaStream_t st) {
     if (precision == 1) {
-        switch (K) {
-            PD_DISPATCH_FP64(16)
-            PD_DISPATCH_FP64(32)
-            default: return cudaErrorInvalidValue;
-        }
+        PD_F64(16, 0) PD_F64(16, 1) PD_F64(32, 0) PD_F64(32, 1)
+        return cudaErrorInvalidValue;
     }
-    switch (K) {
-        PD_DISPATCH_FP32(32)
-        PD_DISPATCH_FP32(64)
-        PD_DISPATCH_FP32(96)
-        PD_DISPATCH_FP32(128)
-        default: return cudaErrorInvalidValue;
-    }
+    PD_F32(32, 0, 4) PD_F32(64, 0, 2) PD_F32(64, 0, 4) PD_F32(96, 0, 2) PD_F32(128, 0, 2)
+    PD_F32(128, 0, 4) PD_F32(32, 1, 2) PD_F32(64, 1, 2)
+    return cudaErrorInvalidValue;
 }
 
-int pairs_blocks_per_sm(int precision, int K, int mode) {
-    const bool c = mode == PD_MODE_CLASS;
+#define PD_O32(K, M, NP) \
+    if (K_ == K && mode == M && NP_ == NP) return occupancy_fp32<K, M, NP>();
+#define PD_O64(K, M) \
+    if (K_ == K && mode == M) return occupancy_fp64<K, M>();
+
+int pairs_blocks_per_sm(int precision, int K_, int NP_, int mode) {
     if (precision == 1) {
-        switch (K) {
-            case 16: return c ? occupancy_fp64<16, 0>() : occupancy_fp64<16, 1>();
-            case 32: return c ? occupancy_fp64<32, 0>() : occupancy_fp64<32, 1>();
-            default: return 0;
-        }
+        PD_O64(16, 0) PD_O64(16, 1) PD_O64(32, 0) PD_O64(32, 1)
+        return 0;
     }
-    switch (K) {
-        case 32: return c ? occupancy_fp32<32, 0>() : occupancy_fp32<32, 1>();
-        case 64: return c ? occupancy_fp32<64, 0>() : occupancy_fp32<64, 1>();
-        case 96: return c ? occupancy_fp32<96, 0>() : occupancy_fp32<96, 1>();
-        case 128: return c ? occupancy_fp32<128, 0>() : occupancy_fp32<128, 1>();
-        default: return 0;
-    }
+    PD_O32(32, 0, 4) PD_O32(64, 0, 2) PD_O32(64, 0, 4) PD_O32(96, 0, 2) PD_O32(128, 0, 2)
+    PD_O32(128, 0, 4) PD_O32(32, 1, 2) PD_O32(64, 1, 2)
+    return 0;
 }
 
 cudaError_t launch_centroid(const double *xyz, int64_t n_atoms, int n_frames, double *centroid,
-                            cudaStream_t st) {
-    pd_centroid<<<n_frames, 256, 0, st>>>(xyz, n_atoms, centroid);
+                            double *radius, cudaStream_t st) {
+    pd_centroid<<<n_frames, 256, 0, st>>>(xyz, n_atoms, centroid, radius);
     return cudaGetLastError();
 }
 
@@ -606,11 +664,13 @@ cudaError_t launch_pack(const double *xyz, const double *weights, const int32_t 
 cudaError_t launch_reduce(const double *slots, const int64_t *lptr, const int64_t *lidx,
                           const PdPairDev *pairs, const double *qv, int32_t n_pairs, int32_t nq,
                           int32_t K, int32_t nv, int32_t n_frames, int64_t slots_per_frame,
+                          const double *radius, double qmin, double dq, int residual_form,
                           double *pairsum, cudaStream_t st) {
     const int64_t total = static_cast<int64_t>(n_pairs) * nq * n_frames;
     const int grid = static_cast<int>((total + 127) / 128);
     pd_reduce_pairs<<<grid, 128, 0, st>>>(slots, lptr, lidx, pairs, qv, n_pairs, nq, K, nv,
-                                          n_frames, slots_per_frame, pairsum);
+                                          n_frames, slots_per_frame, radius, qmin, dq,
+                                          residual_form, pairsum);
     return cudaGetLastError();
 }
 

@@ -10,19 +10,22 @@
 namespace pd {
 
 bool valid_q_block(int precision, int K);
-int pairs_blocks_per_sm(int precision, int K, int mode);
+bool valid_shape(int precision, int mode, int K, int NP);
+int pairs_blocks_per_sm(int precision, int K, int NP, int mode);
 
 // n_jobs points to the tile count in device memory (read once per CTA).
-cudaError_t launch_pairs(int precision, int K, int mode, const PdJob *jobs, const int *n_jobs,
-                         const PdReqDev *reqs, int *counter, int grid, cudaStream_t st);
+cudaError_t launch_pairs(int precision, int K, int NP, int mode, const PdJob *jobs,
+                         const int *n_jobs, const PdReqDev *reqs, int *counter, int grid,
+                         cudaStream_t st);
 cudaError_t launch_centroid(const double *xyz, int64_t n_atoms, int n_frames, double *centroid,
-                            cudaStream_t st);
+                            double *radius, cudaStream_t st);
 cudaError_t launch_pack(const double *xyz, const double *weights, const int32_t *perm,
                         const double *centroid, int64_t n_atoms, int32_t n_pad, int32_t n_frames,
                         float4 *out32, double4 *out64, cudaStream_t st);
 cudaError_t launch_reduce(const double *slots, const int64_t *lptr, const int64_t *lidx,
                           const PdPairDev *pairs, const double *qv, int32_t n_pairs, int32_t nq,
                           int32_t K, int32_t nv, int32_t n_frames, int64_t slots_per_frame,
+                          const double *radius, double qmin, double dq, int residual_form,
                           double *pairsum, cudaStream_t st);
 cudaError_t launch_combine(const double *pairsum, const PdClassDev *cls, const PdPairDev *pairs,
                            int32_t n_cls, int32_t n_pairs, int32_t nq, int32_t nv,

@@ -28,7 +28,7 @@ uint64_t Plan::device_bytes() const {
     const uint64_t lists = (lptr.size() + lidx.size()) * sizeof(int64_t);
     const uint64_t sums = static_cast<uint64_t>(n_frames) * nv * n_pairs * nq * sizeof(double);
     const uint64_t terms = static_cast<uint64_t>(n_frames + 1) * 6 * nq * sizeof(double);
-    const uint64_t misc = static_cast<uint64_t>(n_frames) * 4 * sizeof(double) + 4096;
+    const uint64_t misc = static_cast<uint64_t>(n_frames) * 5 * sizeof(double) + 4096;
     return atoms + xyz_in + tables + layout + jb + slots + lists + sums + terms + misc;
 }
 
@@ -144,9 +144,11 @@ Tuning default_tuning(int64_t n_atoms, int64_t nq, int precision) {
     Tuning t;
     if (precision == PD_FP64) {
         t.K = 32;
+        t.NP = 1;
         t.TJ = std::clamp(next_pow2(n_atoms / 16), 256, 4096);
         return t;
     }
+    t.NP = 2;
     // Longest block that wastes at most ~12 % of a short q grid.
     t.K = 128;
     for (int k : {128, 96, 64}) {
@@ -172,7 +174,8 @@ int build_plan(const pd_request *req, const uint32_t *species, const double *w,
     P.has_exc = req->ff_excluded != nullptr;
     P.has_hyd = req->hyd_weights != nullptr;
     P.tun = tun;
-    if (!valid_q_block(P.precision, tun.K) || tun.TJ < 32 || tun.TJ % 32 != 0) {
+    if (!valid_q_block(P.precision, tun.K) || tun.TJ < 32 || tun.TJ % 32 != 0 ||
+        tun.NP < 1 || tun.NP > 4) {
         msg = "invalid tuning (q block " + std::to_string(tun.K) + ", j chunk " +
               std::to_string(tun.TJ) + ")";
         return PD_EINVAL;
@@ -205,9 +208,18 @@ int build_plan(const pd_request *req, const uint32_t *species, const double *w,
     }
     P.mode = (P.has_hyd && !by_weight) ? PD_MODE_WEIGHTED : PD_MODE_CLASS;
     P.nv = P.mode == PD_MODE_WEIGHTED ? 4 : 1;
-    // Two accumulators per q: longer q blocks than 64 spill registers.
-    if (P.mode == PD_MODE_WEIGHTED && P.precision == PD_FP32_FP64RED && P.tun.K > 64)
-        P.tun.K = 64;
+    // Fit the requested shape to an instantiated kernel: two accumulators per q
+    // (weighted mode) allow q blocks up to 64; FP64 runs one pair per pass.
+    if (P.precision == PD_FP64) {
+        P.tun.NP = 1;
+    } else if (!valid_shape(P.precision, P.mode, P.tun.K, P.tun.NP)) {
+        if (P.mode == PD_MODE_WEIGHTED) {
+            P.tun.K = P.tun.K > 32 ? 64 : 32;
+            P.tun.NP = 2;
+        } else {
+            P.tun.NP = P.tun.K == 32 ? 4 : 2;
+        }
+    }
     int c = 0;
     for (auto &kv : keys) kv.second = c++;
     P.n_cls = c;

@@ -17,6 +17,7 @@ constexpr int PD_MAX_CLASSES = 48;
 struct Tuning {
     int K = 64;     // q-block length
     int TJ = 2048;  // j atoms per tile
+    int NP = 2;     // pairs per thread per pass (FP32 form; 1 for FP64)
 };
 
 struct Plan {

@@ -112,6 +112,10 @@ def surface_distance(p: np.ndarray, axes) -> np.ndarray:
     a2 = a * a
     if np.allclose(a, a[0, 0]):
         return a[0, 0] - np.linalg.norm(p, axis=1)
+    # A zero coordinate on a shorter axis puts the root at the pole t = -a²
+    # (closest points off that axis); a 1e-6 Å nudge moves it inside the
+    # bracket at a distance error of ~1e-6 Å.
+    p = np.where(p == 0.0, 1e-6, p)
     lo = np.full(len(p), -a2.min() * (1.0 - 1e-15))
     hi = np.zeros(len(p))
     for _ in range(100):

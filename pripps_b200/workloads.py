@@ -105,6 +105,15 @@ def ellipsoid_solvent_100k(precision="fp32") -> Workload:
                     globule_request(g, 0.0, 1.0, 1000, True, precision), g)
 
 
+def ellipsoid_solvent_20k(precision="fp32") -> Workload:
+    """A fifth of the 100k workload at the same density (axes × 0.2^{1/3}),
+    nq = 512: the size used for detailed kernel profiles."""
+    f = 0.2 ** (1.0 / 3.0)
+    g = _globule(20_000, (80.0 * f, 40.0 * f, 40.0 * f), 12)
+    return Workload("ellipsoid_solvent_20k",
+                    globule_request(g, 0.0, 1.0, 512, True, precision), g)
+
+
 def trajectory_5k_256(precision="fp32", n_frames: int = 256) -> Workload:
     g = _globule(5000, (25.0, 25.0, 25.0), 3)
     frames, w = synth.trajectory(g.pos, n_frames, 0.5, 3)
@@ -130,5 +139,6 @@ WORKLOADS = {
     "sphere_vacuum_1k": sphere_vacuum_1k,
     "sphere_solvent_10k": sphere_solvent_10k,
     "ellipsoid_solvent_100k": ellipsoid_solvent_100k,
+    "ellipsoid_solvent_20k": ellipsoid_solvent_20k,
     "trajectory_5k_256": trajectory_5k_256,
 }
