@@ -75,10 +75,15 @@ __device__ __forceinline__ void sincos_reduced(float th, float &s, float &c) {
     c = ((qd + 1) & 2) ? -cc : cc;
 }
 
-// Seed of one pair for a q-block: the recurrence state (u, d), the negated
-// step coefficient -α and the weights for even and odd steps (σ^k folded in).
+// Seed of one pair for a q-block. The K values s_k = sin(θ + k x), θ = q_s r,
+// x = Δq r, are produced as two interleaved sequences, even k and odd k, each
+// a sinusoid in j = k/2 with step y = 2x: s_{2j} = sin(θ + j y) and
+// s_{2j+1} = sin(θ + x + j y). With y = mπ + y' (|y'| <= π/2) and σ = (-1)^m,
+// both are σ^j·v_j where v follows the Reinsch recurrence with
+// α = 4 sin²(y'/2). Two independent chains per pair halve the dependency
+// stall of the FFMA → FADD step without adding instructions.
 struct PairSeed {
-    float u, d, na, we, wo;
+    float ve, de, vo, dd, na, we, wo;
 };
 
 __device__ __forceinline__ PairSeed pair_seed(float4 pi, float4 pj, bool valid, float qs_hi,
@@ -90,47 +95,58 @@ __device__ __forceinline__ PairSeed pair_seed(float4 pi, float4 pj, bool valid, 
     r2 = fmaxf(r2, 1e-12f);
     const float inv_r = rsqrtf(r2);
     float r = r2 * inv_r;
-    r = fmaf(0.5f * inv_r, fmaf(-r, r, r2), r);  // one Newton step on sqrt
-    const float x = fmaf(dq_hi, r, dq_lo * r);   // Δq·r
-    const float th = fmaf(qs_hi, r, qs_lo * r);  // q_s·r
-    // x = mπ + x', |x'| <= π/2 (two-part π: 3.140625 + 9.67653589793e-4).
-    const float m = rintf(x * 0.318309886f);
-    float xr = fmaf(-m, 3.140625f, x);
-    xr = fmaf(-m, 9.67653589793e-4f, xr);
-    const float sgn = (static_cast<int>(m) & 1) ? -1.0f : 1.0f;
-    const float h = 0.5f * xr;
+    r = fmaf(0.5f * inv_r, fmaf(-r, r, r2), r);   // one Newton step on sqrt
+    const float y = 2.0f * fmaf(dq_hi, r, dq_lo * r);  // 2Δq·r (exact doubling)
+    const float th = fmaf(qs_hi, r, qs_lo * r);        // q_s·r
+    // y = mπ + y', |y'| <= π/2 (two-part π: 3.140625 + 9.67653589793e-4).
+    const float m = rintf(y * 0.318309886f);
+    float yr = fmaf(-m, 3.140625f, y);
+    yr = fmaf(-m, 9.67653589793e-4f, yr);
+    const int mi = static_cast<int>(m);
+    const float h = 0.5f * yr;  // x = m·π/2 + h
     const float sh = sin_small(h), ch = cos_small(h);
+    // sin x, cos x from the quadrant of m
+    const bool swap = (mi & 1) != 0;
+    float sx = swap ? ch : sh;
+    float cx = swap ? sh : ch;
+    sx = (mi & 2) ? -sx : sx;
+    cx = ((mi + 1) & 2) ? -cx : cx;
     float s0, c0;
     sincos_reduced(th, s0, c0);
+    const float s1 = fmaf(s0, cx, c0 * sx);   // sin(θ + x)
+    const float c1 = fmaf(c0, cx, -s0 * sx);  // cos(θ + x)
+    const float sh2 = 2.0f * sh;
     PairSeed ps;
-    ps.u = s0;                                 // u_0 = sin θ
-    ps.d = 2.0f * sh * fmaf(c0, ch, s0 * sh);  // u_0 − u_{−1} = 2 sin h cos(θ − h)
-    ps.na = -4.0f * sh * sh;                   // −α
+    ps.ve = s0;                                // v_0 even = sin θ
+    ps.de = sh2 * fmaf(c0, ch, s0 * sh);       // sin θ − sin(θ − y') = 2 sin h cos(θ − h)
+    ps.vo = s1;                                // v_0 odd = sin(θ + x)
+    ps.dd = sh2 * fmaf(c1, ch, s1 * sh);
+    ps.na = -sh2 * sh2;                        // −α = −4 sin² h
     const float w = valid ? inv_r : 0.0f;
     ps.we = w;
-    ps.wo = sgn * w;
+    ps.wo = (mi & 1) ? -w : w;
     return ps;
 }
 
-// A q-block uses the residual form when q_s·(2·radius) < 4: there the terms
-// sin(q r)/r are all close to q, and accumulating them directly in FP32 would
-// round with a systematic bias; the kernel accumulates sin(q r)/r − q instead
-// and the reduction adds (pair count)·q back in FP64. Both kernels evaluate
-// this predicate from the same FP64 inputs.
-__host__ __device__ __forceinline__ bool residual_block(int qb, int K, double qmin, double dq,
-                                                        double radius) {
-    const double qs = qmin + static_cast<double>(qb) * K * dq;
-    return qs * (2.0 * radius) < 4.0;
+// Small-q residual form: where q·(2·radius) < 2 every pair has q·r < 2 and
+// the terms sin(q r)/r lie within a factor 0.45..1 of q, so a sequential FP32
+// sum of them rounds with a systematic bias. There the kernel accumulates
+// sin(q r)/r − q and the reduction adds (pair count)·q back in FP64. Both
+// kernels evaluate this predicate on the same FP64 values.
+__host__ __device__ __forceinline__ bool residual_q(double q, double radius) {
+    return q * (2.0 * radius) < 2.0;
 }
 
 // ---------------------------------------------------------------- K1 (FP32)
-// NP pairs per thread per pass: independent recurrence chains for ILP.
+// NP pairs per thread per pass, two chains each: 2·NP independent recurrences.
 template <int K, int MODE, int NP, bool RESID>
 __device__ __forceinline__ void pairs_range(const float4 *__restrict__ at, float4 pi, int i,
                                             bool ivalid, int j0, int j1, float qs_hi,
                                             float qs_lo, float dq_hi, float dq_lo,
+                                            const float *__restrict__ s_qres,
                                             float (&acc)[(MODE == PD_MODE_WEIGHTED) ? 2 : 1][K]) {
     constexpr int NACC = (MODE == PD_MODE_WEIGHTED) ? 2 : 1;
+    static_assert(K % 4 == 0, "K must be a multiple of 4");
     for (int j = j0; j < j1; j += NP) {
         PairSeed S[NP];
         float wj[NP];
@@ -148,11 +164,6 @@ __device__ __forceinline__ void pairs_range(const float4 *__restrict__ at, float
                 if (MODE == PD_MODE_WEIGHTED) vwsum += valid ? pj.w : 0.0f;
             }
         }
-        // q_k = q_s + k·Δq is the same in every pass of this loop; passing q_s
-        // through an opaque move keeps the compiler from hoisting all K values
-        // into registers.
-        float qs_pass = qs_hi;
-        if (RESID) asm volatile("mov.b32 %0, %0;" : "+f"(qs_pass));
         float we_w[NP], wo_w[NP];
         if (MODE == PD_MODE_WEIGHTED) {
 #pragma unroll
@@ -161,39 +172,54 @@ __device__ __forceinline__ void pairs_range(const float4 *__restrict__ at, float
                 wo_w[p] = S[p].wo * wj[p];
             }
         }
+        // The q table is the same in every pass; an opaque zero offset keeps
+        // the compiler from hoisting all K loads into registers.
+        int qoff = 0;
+        if (RESID) asm volatile("mov.b32 %0, %0;" : "+r"(qoff));
 #pragma unroll
-        for (int k = 0; k < K; k += 2) {
+        for (int k = 0; k < K; k += 4) {
 #pragma unroll
-            for (int h = 0; h < 2; ++h) {
+            for (int h = 0; h < 4; ++h) {
+                const int kk = k + h;
+                const bool odd_chain = (h & 1) != 0;  // k = 4t+1, 4t+3
+                const bool odd_j = (h & 2) != 0;      // j = 2t+1: weight σ·w
                 if (RESID) {
-                    const float qk = fmaf(static_cast<float>(k + h), dq_hi, qs_pass);
-                    acc[0][k + h] = fmaf(-vsum, qk, acc[0][k + h]);
+                    const float qk = s_qres[kk + qoff];
+                    acc[0][kk] = fmaf(-vsum, qk, acc[0][kk]);
                     if (MODE == PD_MODE_WEIGHTED)
-                        acc[NACC - 1][k + h] = fmaf(-vwsum, qk, acc[NACC - 1][k + h]);
+                        acc[NACC - 1][kk] = fmaf(-vwsum, qk, acc[NACC - 1][kk]);
                 }
 #pragma unroll
                 for (int p = 0; p < NP; ++p) {
-                    const float w = h ? S[p].wo : S[p].we;
-                    acc[0][k + h] = fmaf(w, S[p].u, acc[0][k + h]);
+                    const float w = odd_j ? S[p].wo : S[p].we;
+                    float &v = odd_chain ? S[p].vo : S[p].ve;
+                    float &d = odd_chain ? S[p].dd : S[p].de;
+                    acc[0][kk] = fmaf(w, v, acc[0][kk]);
                     if (MODE == PD_MODE_WEIGHTED)
-                        acc[NACC - 1][k + h] =
-                            fmaf(h ? wo_w[p] : we_w[p], S[p].u, acc[NACC - 1][k + h]);
-                    S[p].d = fmaf(S[p].na, S[p].u, S[p].d);
-                    S[p].u += S[p].d;
+                        acc[NACC - 1][kk] = fmaf(odd_j ? wo_w[p] : we_w[p], v, acc[NACC - 1][kk]);
+                    d = fmaf(S[p].na, v, d);
+                    v += d;
                 }
             }
         }
     }
 }
 
+// Resident CTAs per SM each FP32 shape is compiled for (register budget
+// 65536 / (128 · blocks) per thread).
+constexpr int fp32_min_blocks(int K, int MODE, int NP) {
+    return MODE == PD_MODE_CLASS ? (K <= 64 ? 4 : (NP == 2 ? 3 : 2)) : (K <= 32 ? 4 : 2);
+}
+
 template <int K, int MODE, int NP>
-__global__ void __launch_bounds__(PD_THREADS) pd_pairs_fp32(const PdJob *__restrict__ jobs,
+__global__ void __launch_bounds__(PD_THREADS, fp32_min_blocks(K, MODE, NP))
+    pd_pairs_fp32(const PdJob *__restrict__ jobs,
                                                             const int *__restrict__ n_jobs_ptr,
                                                             const PdReqDev *__restrict__ reqs,
                                                             int *__restrict__ counter) {
-    static_assert(K % 2 == 0, "K must be even");
     constexpr int NACC = (MODE == PD_MODE_WEIGHTED) ? 2 : 1;
     __shared__ int s_job;
+    __shared__ float s_qres[K];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const int n_jobs = *n_jobs_ptr;
@@ -201,15 +227,23 @@ __global__ void __launch_bounds__(PD_THREADS) pd_pairs_fp32(const PdJob *__restr
         if (threadIdx.x == 0) s_job = atomicAdd(counter, 1);
         __syncthreads();
         const int jid = s_job;
-        __syncthreads();
         if (jid >= n_jobs) break;
         const PdJob jb = jobs[jid];
         const PdReqDev rq = reqs[jb.req];
+        const int kq0 = jb.qb * K;
+        const double radius = rq.radius[jb.frame];
+        const bool resid = kq0 < rq.nq && residual_q(rq.qv[kq0], radius);
+        if (resid && threadIdx.x < K) {
+            const int kq = kq0 + threadIdx.x;
+            const bool on = kq < rq.nq && residual_q(rq.qv[kq], radius);
+            s_qres[threadIdx.x] = on ? static_cast<float>(rq.qv[kq]) : 0.0f;
+        }
+        __syncthreads();  // s_qres ready; every thread has read s_job
         const float4 *__restrict__ at = rq.atoms32 + static_cast<size_t>(jb.frame) * rq.n_pad;
         const int i = jb.i0 + threadIdx.x;
         const float4 pi = at[i];
         const bool ivalid = lane < rq.gvalid[(jb.i0 >> 5) + warp];
-        const double qs = rq.qmin + static_cast<double>(jb.qb * K) * rq.dq;
+        const double qs = rq.qmin + static_cast<double>(kq0) * rq.dq;
         const float qs_hi = static_cast<float>(qs);
         const float qs_lo = static_cast<float>(qs - static_cast<double>(qs_hi));
         const float dq_hi = static_cast<float>(rq.dq);
@@ -221,12 +255,12 @@ __global__ void __launch_bounds__(PD_THREADS) pd_pairs_fp32(const PdJob *__restr
 #pragma unroll
             for (int k = 0; k < K; ++k) acc[a][k] = 0.0f;
 
-        if (residual_block(jb.qb, K, rq.qmin, rq.dq, rq.radius[jb.frame]))
+        if (resid)
             pairs_range<K, MODE, NP, true>(at, pi, i, ivalid, jb.j0, jb.j1, qs_hi, qs_lo, dq_hi,
-                                           dq_lo, acc);
+                                           dq_lo, s_qres, acc);
         else
             pairs_range<K, MODE, NP, false>(at, pi, i, ivalid, jb.j0, jb.j1, qs_hi, qs_lo, dq_hi,
-                                            dq_lo, acc);
+                                            dq_lo, s_qres, acc);
 
         // Warp-reduce and write this warp's slot: [nv][K] FP64 values.
         double *slot = rq.slots + (jb.slot + warp) * static_cast<int64_t>(K) *
@@ -253,6 +287,7 @@ __global__ void __launch_bounds__(PD_THREADS) pd_pairs_fp32(const PdJob *__restr
                 }
             }
         }
+        __syncthreads();  // s_qres and s_job are rewritten by the next tile
     }
 }
 
@@ -432,7 +467,7 @@ __global__ void pd_reduce_pairs(const double *__restrict__ slots, const int64_t 
             for (int v = 0; v < nv; ++v) s[v] += sl[v * K + kk];
         }
         for (int v = 0; v < nv; ++v) s[v] /= qval;
-        if (residual_form && residual_block(qb, K, qmin, dq, radius[f]))
+        if (residual_form && residual_q(qval, radius[f]))
             for (int v = 0; v < nv; ++v) s[v] += pairs[p].q0[v];
     } else {
         for (int v = 0; v < 4; ++v) s[v] = pairs[p].q0[v];

@@ -148,18 +148,30 @@ Tuning default_tuning(int64_t n_atoms, int64_t nq, int precision) {
         t.TJ = std::clamp(next_pow2(n_atoms / 16), 256, 4096);
         return t;
     }
-    t.NP = 2;
-    // Longest block that wastes at most ~12 % of a short q grid.
-    t.K = 128;
-    for (int k : {128, 96, 64}) {
-        const int64_t nb = (nq + k - 1) / k;
-        if (nb * k - nq <= std::max<int64_t>(nq / 8, 0) || k == 64) {
-            t.K = k;
-            break;
+    // Measured on B200 (class mode): K = 128 with 2 pairs per thread is the
+    // fastest shape from ~4k atoms up, K = 64 with 4 pairs below; a j chunk of
+    // about N/8 atoms balances tile count against per-tile overhead.
+    if (n_atoms < 4000) {
+        t.K = 64;
+        t.NP = 4;
+    } else {
+        // longest block that wastes at most ~12 % of the q grid
+        t.K = 64;
+        t.NP = 4;
+        for (int k : {128, 96}) {
+            const int64_t nb = (nq + k - 1) / k;
+            if (nb * k - nq <= nq / 8) {
+                t.K = k;
+                t.NP = 2;
+                break;
+            }
         }
     }
-    if (nq <= 32) t.K = 32;
-    t.TJ = std::clamp(next_pow2(n_atoms / 8), 512, 8192);
+    if (nq <= 32) {
+        t.K = 32;
+        t.NP = 4;
+    }
+    t.TJ = std::clamp(next_pow2(n_atoms / 8), 256, 16384);
     return t;
 }
 
