@@ -138,6 +138,21 @@ int pd_plan_info(const pd_plan *plan, uint32_t *q_block, uint32_t *j_chunk,
                  uint32_t *pairs_per_thread, uint64_t *n_tiles, uint64_t *device_bytes,
                  uint64_t *upload_bytes);
 
+/* Multi-GPU: restrict a plan to rank's share of the tiles (every world-th
+ * tile in cost order). Each execution then yields partial profiles whose sum
+ * over the ranks is the full [6][nq] result — rank 0 also carries the i = j
+ * terms and the exact q = 0 sums — so the caller adds them across devices
+ * (one all-reduce of 6·nq doubles). world = 1 restores the whole plan. No
+ * reference counterpart (the reference is single-process). */
+int pd_plan_set_shard(pd_ctx *ctx, pd_plan *plan, uint32_t rank, uint32_t world);
+
+/* Host-only view of a request's tiles in rank's share: five int32 per tile
+ * (first i of the 128-atom block, j range [j0, j1), q-block, frame) in padded
+ * atom indices, and the padded-index -> atom permutation (-1 = padding). */
+int pd_plan_tiles(pd_ctx *ctx, const pd_request *req, uint32_t rank, uint32_t world,
+                  int32_t *tiles, uint64_t cap, uint64_t *n_tiles, int32_t *perm,
+                  uint64_t perm_cap, uint64_t *n_padded);
+
 /* Kernel timing: with profiling enabled every pd_plan_execute brackets its
  * pair kernel with CUDA events on the execution stream; pd_plan_pair_kernel_ms
  * waits for them and reports the summed duration and the number of timed

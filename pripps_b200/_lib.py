@@ -69,6 +69,10 @@ SIGNATURES = {
     "pd_plan_set_profiling": (C.c_int, [_P, _P, C.c_int]),
     "pd_plan_pair_kernel_ms": (C.c_int, [_P, _P, _D, _U64P]),
     "pd_plan_destroy": (None, [_P, _P]),
+    "pd_plan_set_shard": (C.c_int, [_P, _P, C.c_uint32, C.c_uint32]),
+    "pd_plan_tiles": (C.c_int, [_P, C.POINTER(PdRequest), C.c_uint32, C.c_uint32,
+                                C.POINTER(C.c_int32), C.c_uint64, _U64P, C.POINTER(C.c_int32),
+                                C.c_uint64, _U64P]),
     "pd_submit": (C.c_int, [_P, C.POINTER(PdRequest), _U64P]),
     "pd_wait": (C.c_int, [_P, C.c_uint64, C.c_int, _D]),
     "pd_poll": (C.c_int, [_P, C.c_uint64]),

@@ -156,6 +156,9 @@ struct DevPlan {
     uint64_t charged = 0;
     bool host_xyz = false;
     const double *xyz_dev = nullptr;  // coordinates used by pack
+    // Tile share of a multi-GPU solve: the tiles in the device job list are
+    // this rank's; rank 0 adds the i = j terms and the exact q = 0 sums.
+    uint32_t rank = 0, world = 1;
     template <class T>
     T *dptr(uint64_t off) const {
         return reinterpret_cast<T *>(base + off);
@@ -313,13 +316,13 @@ int finish_devplan(pd_ctx *ctx, DevPlan &dp, double *out_dev, cudaStream_t st) {
                                    dp.dptr<double>(L.qv), P.n_pairs, P.nq, P.tun.K, P.nv,
                                    P.n_frames, P.slots_per_frame, dp.dptr<double>(L.radius),
                                    P.qmin, P.dq, P.precision == PD_FP32_FP64RED ? 1 : 0,
-                                   dp.dptr<double>(L.pairsum), st));
+                                   dp.rank == 0 ? 1 : 0, dp.dptr<double>(L.pairsum), st));
     PD_CUDA(ctx, pd::launch_combine(dp.dptr<double>(L.pairsum), dp.dptr<PdClassDev>(L.cls),
                                     dp.dptr<PdPairDev>(L.pairs), P.n_cls, P.n_pairs, P.nq, P.nv,
                                     P.n_frames, dp.dptr<double>(L.ffA),
                                     P.has_exc ? dp.dptr<double>(L.ffC) : nullptr,
                                     P.has_hyd ? dp.dptr<double>(L.ffW) : nullptr,
-                                    dp.dptr<double>(L.terms), st));
+                                    dp.rank == 0 ? 1 : 0, dp.dptr<double>(L.terms), st));
     ctx->launches += 2;
     double *dst = out_dev ? out_dev : dp.dptr<double>(L.out);
     if (P.n_frames > 1) {
@@ -365,12 +368,18 @@ int run_devplan(pd_ctx *ctx, DevPlan &dp, double *out_dev, cudaStream_t st,
     int rc = pack_devplan(ctx, dp, st);
     if (rc) return rc;
     if (ev) cudaEventRecord(ev->first, st);
+    if (dp.world > 1)  // the lists also name the other ranks' slots
+        PD_CUDA(ctx, cudaMemsetAsync(dp.dptr<double>(L.slots), 0,
+                                     static_cast<size_t>(P.slots_per_frame) * P.n_frames * P.nv *
+                                         P.tun.K * 8,
+                                     st));
     if (!P.jobs.empty()) {
         PD_CUDA(ctx, cudaMemsetAsync(dp.dptr<int>(L.counter), 0, sizeof(int), st));
         PD_CUDA(ctx, pd::launch_pairs(P.precision, P.tun.K, P.tun.NP, P.mode, dp.dptr<PdJob>(L.jobs),
                                       dp.dptr<int>(L.njobs), dp.dptr<PdReqDev>(L.req),
                                       dp.dptr<int>(L.counter),
-                                      persistent_grid(ctx, P, static_cast<int64_t>(P.jobs.size())),
+                                      persistent_grid(ctx, P, static_cast<int64_t>(P.jobs.size()) /
+                                                                  static_cast<int64_t>(dp.world) + 1),
                                       st));
         ctx->launches += 1;
     }
@@ -949,6 +958,63 @@ int pd_plan_info(const pd_plan *plan, uint32_t *q_block, uint32_t *j_chunk, uint
     if (j_chunk) *j_chunk = static_cast<uint32_t>(plan->dp.P.tun.TJ);
     if (n_tiles) *n_tiles = plan->dp.P.jobs.size();
     if (device_bytes) *device_bytes = plan->dp.L.total;
+    return PD_OK;
+}
+
+int pd_plan_set_shard(pd_ctx *ctx, pd_plan *plan, uint32_t rank, uint32_t world) {
+    if (!ctx || !plan || world == 0 || rank >= world) return PD_EINVAL;
+    std::lock_guard<std::mutex> g(ctx->solve_mu);
+    cudaSetDevice(ctx->device);
+    DevPlan &dp = plan->dp;
+    // every world-th tile in execution (cost) order
+    std::vector<PdJob> mine;
+    mine.reserve(dp.P.jobs.size() / world + 1);
+    for (size_t t = rank; t < dp.P.jobs.size(); t += world) mine.push_back(dp.P.jobs[t]);
+    const int nj = static_cast<int>(mine.size());
+    PD_CUDA(ctx, cudaMemcpyAsync(dp.dptr<PdJob>(dp.L.jobs), mine.data(), mine.size() * sizeof(PdJob),
+                                 cudaMemcpyHostToDevice, ctx->stream));
+    PD_CUDA(ctx, cudaMemcpyAsync(dp.dptr<int>(dp.L.njobs), &nj, sizeof(int), cudaMemcpyHostToDevice,
+                                 ctx->stream));
+    PD_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    dp.rank = rank;
+    dp.world = world;
+    return PD_OK;
+}
+
+int pd_plan_tiles(pd_ctx *ctx, const pd_request *req, uint32_t rank, uint32_t world,
+                  int32_t *tiles, uint64_t cap, uint64_t *n_tiles, int32_t *perm,
+                  uint64_t perm_cap, uint64_t *n_padded) {
+    if (!req || world == 0 || rank >= world) return PD_EINVAL;
+    std::string msg;
+    int rc = pd::validate_request(req, false, msg);
+    if (rc) {
+        if (ctx) ctx->set_error(msg);
+        return rc;
+    }
+    Tuning tun = tuning_for(ctx, static_cast<int64_t>(req->n_atoms), static_cast<int64_t>(req->nq),
+                            static_cast<int>(req->precision));
+    Plan P;
+    rc = pd::build_plan(req, req->species, req->hyd_weights, tun, P, msg);
+    if (rc) {
+        if (ctx) ctx->set_error(msg);
+        return rc;
+    }
+    uint64_t n = 0;
+    for (size_t t = rank; t < P.jobs.size(); t += world, ++n) {
+        if (tiles && n < cap) {
+            int32_t *o = tiles + 5 * n;
+            o[0] = P.jobs[t].i0;
+            o[1] = P.jobs[t].j0;
+            o[2] = P.jobs[t].j1;
+            o[3] = P.jobs[t].qb;
+            o[4] = P.jobs[t].frame;
+        }
+    }
+    if (n_tiles) *n_tiles = n;
+    if (perm && perm_cap >= P.perm.size())
+        std::memcpy(perm, P.perm.data(), P.perm.size() * sizeof(int32_t));
+    if (n_padded) *n_padded = static_cast<uint64_t>(P.n_pad);
+    if (tiles && n > cap) return PD_ENOMEM;
     return PD_OK;
 }
 

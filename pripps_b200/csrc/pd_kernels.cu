@@ -39,33 +39,54 @@ __device__ __forceinline__ double warp_sum(double v) {
     return v;
 }
 
-// sin and cos on |h| <= π/4 from their Taylor series (truncation error below
-// 3e-9 there, under the FP32 rounding of the result).
+// sin and cos on |h| <= π/4 as polynomials in h² whose FP32 coefficients were
+// fitted (least squares on Chebyshev nodes, each coefficient rounded to FP32
+// before the next ones were refitted): |error| < 4e-11 for sin and < 1e-11
+// for cos on the interval, in exact arithmetic, far under the FP32 rounding
+// of the result. Taylor coefficients rounded to FP32 leave a one-signed
+// error of ~1e-9, which a sum over 10^8 pairs turns into a bias.
 __device__ __forceinline__ float sin_small(float h) {
     const float h2 = h * h;
-    float p = 2.7557319e-6f;                 //  1/9!
-    p = fmaf(p, h2, -1.9841270e-4f);         // -1/7!
-    p = fmaf(p, h2, 8.3333333e-3f);          //  1/5!
-    p = fmaf(p, h2, -1.6666667e-1f);         // -1/3!
+    float p = -2.597475088e-7f;
+    p = fmaf(p, h2, 3.148236829e-6f);
+    p = fmaf(p, h2, -1.986468124e-4f);
+    p = fmaf(p, h2, 8.333391510e-3f);
+    p = fmaf(p, h2, -1.666666716e-1f);
     return fmaf(h * h2, p, h);
 }
 __device__ __forceinline__ float cos_small(float h) {
     const float h2 = h * h;
-    float p = -2.7557319e-7f;                // -1/10!
-    p = fmaf(p, h2, 2.4801587e-5f);          //  1/8!
-    p = fmaf(p, h2, -1.3888889e-3f);         // -1/6!
-    p = fmaf(p, h2, 4.1666667e-2f);          //  1/4!
-    p = fmaf(p, h2, -0.5f);                  // -1/2!
+    float p = -2.870663707e-7f;
+    p = fmaf(p, h2, 2.482019954e-5f);
+    p = fmaf(p, h2, -1.388897537e-3f);
+    p = fmaf(p, h2, 4.166666791e-2f);
+    p = fmaf(p, h2, -0.5f);
     return fmaf(h2, p, 1.0f);
 }
 
-// sin and cos of an FP32 angle |th| <~ 1e4 without a branch: th = n·π/2 + t
-// with a two-part π/2 (1.5703125 is exact in 8 bits, so n·1.5703125 is exact
-// for n < 2^15), then the Taylor forms on |t| <= π/4 and the quadrant of n.
-__device__ __forceinline__ void sincos_reduced(float th, float &s, float &c) {
-    const float n = rintf(th * 0.636619772f);
-    float t = fmaf(-n, 1.5703125f, th);
-    t = fmaf(-n, 4.83826794897e-4f, t);
+// Three-part π/2 for the reduction: C1 has 8 significant bits, so n·C1 and
+// th − n·C1 are exact for n < 2^15; C2 = fl32(π/2 − C1); C3 = fl32(π/2 − C1 − C2).
+constexpr float kPio2C1 = 1.5703125f;
+constexpr float kPio2C2 = 4.838267923333e-4f;
+constexpr float kPio2C3 = 2.563282919255e-12f;
+
+// sin and cos of an angle given as an unevaluated sum th_hi + th_lo
+// (|th_hi| <~ 1e4, |th_lo| a few ulp of th_hi), without a branch:
+// th = n·π/2 + t, t = (th_hi − n·C1) + (th_lo − n·C2 − n·C3), then the
+// polynomials on |t| <= π/4 and the quadrant of n.
+//
+// Why the low part: th_hi lies on the FP32 grid of its binade, and th_hi − n·C1
+// is exact, so rounding (th_hi − n·π/2) to FP32 in one step gives the same
+// rounding error to every pair of that quadrant and binade — a bias of
+// ~2e-9 per sin that survives a sum over 10^7..10^10 pairs. th_lo carries
+// the pair's own rounding residue of q·r, so the final rounding of t falls
+// at a random place between grid points and averages out.
+__device__ __forceinline__ void sincos_reduced(float th_hi, float th_lo, float &s, float &c) {
+    const float n = rintf(th_hi * 0.636619772f);
+    const float t1 = fmaf(-n, kPio2C1, th_hi);  // exact
+    float u = fmaf(-n, kPio2C2, th_lo);
+    u = fmaf(-n, kPio2C3, u);
+    const float t = t1 + u;
     const float st = sin_small(t), ct = cos_small(t);
     const int qd = static_cast<int>(n);
     const bool swap = (qd & 1) != 0;
@@ -86,22 +107,38 @@ struct PairSeed {
     float ve, de, vo, dd, na, we, wo;
 };
 
+// Three-part π for the step reduction (C1 = 3.140625 has 8 significant bits).
+constexpr float kPiC1 = 3.140625f;
+constexpr float kPiC2 = 9.676535846666e-4f;
+constexpr float kPiC3 = 5.126565838511e-12f;
+
 __device__ __forceinline__ PairSeed pair_seed(float4 pi, float4 pj, bool valid, float qs_hi,
-                                              float qs_lo, float dq_hi, float dq_lo) {
+                                              float qs_lo, float dq2_hi, float dq2_lo) {
     const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
     float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
     // Coincident points: sinc(0) = 1, i.e. sin(q r)/r -> q; r = 1e-6 Å gives
     // that limit to 1e-13 relative.
     r2 = fmaxf(r2, 1e-12f);
-    const float inv_r = rsqrtf(r2);
-    float r = r2 * inv_r;
-    r = fmaf(0.5f * inv_r, fmaf(-r, r, r2), r);   // one Newton step on sqrt
-    const float y = 2.0f * fmaf(dq_hi, r, dq_lo * r);  // 2Δq·r (exact doubling)
-    const float th = fmaf(qs_hi, r, qs_lo * r);        // q_s·r
-    // y = mπ + y', |y'| <= π/2 (two-part π: 3.140625 + 9.67653589793e-4).
-    const float m = rintf(y * 0.318309886f);
-    float yr = fmaf(-m, 3.140625f, y);
-    yr = fmaf(-m, 9.67653589793e-4f, yr);
+    float inv_r = rsqrtf(r2);
+    // r = r_hi + r_lo to ~2^-44 relative: one Newton step on sqrt, its
+    // correction kept apart.
+    const float r_hi = r2 * inv_r;
+    const float hinv = 0.5f * inv_r;
+    const float r_lo = hinv * fmaf(-r_hi, r_hi, r2);
+    // One Newton step on 1/r as well: the weight multiplies every term of the
+    // pair, so its error must be unbiased, not just small.
+    inv_r = fmaf(hinv, fmaf(-r2 * inv_r, inv_r, 1.0f), inv_r);
+    // θ = q_s·r and y = 2Δq·r as hi + lo pairs (exact product residue plus the
+    // cross terms of the two double-float factors).
+    const float th_hi = qs_hi * r_hi;
+    const float th_lo = fmaf(qs_hi, r_hi, -th_hi) + fmaf(qs_hi, r_lo, qs_lo * r_hi);
+    const float y_hi = dq2_hi * r_hi;
+    const float y_lo = fmaf(dq2_hi, r_hi, -y_hi) + fmaf(dq2_hi, r_lo, dq2_lo * r_hi);
+    // y = mπ + y', |y'| <= π/2, reduced like θ.
+    const float m = rintf(y_hi * 0.318309886f);
+    float yl = fmaf(-m, kPiC2, y_lo);
+    yl = fmaf(-m, kPiC3, yl);
+    const float yr = fmaf(-m, kPiC1, y_hi) + yl;
     const int mi = static_cast<int>(m);
     const float h = 0.5f * yr;  // x = m·π/2 + h
     const float sh = sin_small(h), ch = cos_small(h);
@@ -112,7 +149,7 @@ __device__ __forceinline__ PairSeed pair_seed(float4 pi, float4 pj, bool valid, 
     sx = (mi & 2) ? -sx : sx;
     cx = ((mi + 1) & 2) ? -cx : cx;
     float s0, c0;
-    sincos_reduced(th, s0, c0);
+    sincos_reduced(th_hi, th_lo, s0, c0);
     const float s1 = fmaf(s0, cx, c0 * sx);   // sin(θ + x)
     const float c1 = fmaf(c0, cx, -s0 * sx);  // cos(θ + x)
     const float sh2 = 2.0f * sh;
@@ -246,8 +283,9 @@ __global__ void __launch_bounds__(PD_THREADS, fp32_min_blocks(K, MODE, NP))
         const double qs = rq.qmin + static_cast<double>(kq0) * rq.dq;
         const float qs_hi = static_cast<float>(qs);
         const float qs_lo = static_cast<float>(qs - static_cast<double>(qs_hi));
-        const float dq_hi = static_cast<float>(rq.dq);
-        const float dq_lo = static_cast<float>(rq.dq - static_cast<double>(dq_hi));
+        const double dq2 = 2.0 * rq.dq;  // step of the even/odd chains
+        const float dq_hi = static_cast<float>(dq2);
+        const float dq_lo = static_cast<float>(dq2 - static_cast<double>(dq_hi));
 
         float acc[NACC][K];
 #pragma unroll
@@ -447,7 +485,8 @@ __global__ void pd_reduce_pairs(const double *__restrict__ slots, const int64_t 
                                 const double *__restrict__ qv, int32_t n_pairs, int32_t nq,
                                 int32_t K, int32_t nv, int32_t n_frames, int64_t slots_per_frame,
                                 const double *__restrict__ radius, double qmin, double dq,
-                                int32_t residual_form, double *__restrict__ pairsum) {
+                                int32_t residual_form, int32_t add_exact,
+                                double *__restrict__ pairsum) {
     const int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
     const int64_t per_frame = static_cast<int64_t>(n_pairs) * nq;
     if (t >= per_frame * n_frames) return;
@@ -467,9 +506,9 @@ __global__ void pd_reduce_pairs(const double *__restrict__ slots, const int64_t 
             for (int v = 0; v < nv; ++v) s[v] += sl[v * K + kk];
         }
         for (int v = 0; v < nv; ++v) s[v] /= qval;
-        if (residual_form && residual_q(qval, radius[f]))
+        if (add_exact && residual_form && residual_q(qval, radius[f]))
             for (int v = 0; v < nv; ++v) s[v] += pairs[p].q0[v];
-    } else {
+    } else if (add_exact) {
         for (int v = 0; v < 4; ++v) s[v] = pairs[p].q0[v];
     }
     const int64_t ob = static_cast<int64_t>(f) * nv * per_frame;
@@ -482,7 +521,8 @@ __global__ void pd_combine_terms(const double *__restrict__ pairsum,
                                  const PdPairDev *__restrict__ pairs, int32_t n_cls,
                                  int32_t n_pairs, int32_t nq, int32_t nv, int32_t n_frames,
                                  const double *__restrict__ ffA, const double *__restrict__ ffC,
-                                 const double *__restrict__ ffW, double *__restrict__ terms) {
+                                 const double *__restrict__ ffW, int32_t add_diag,
+                                 double *__restrict__ terms) {
     const int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
     if (t >= static_cast<int64_t>(nq) * n_frames) return;
     const int f = static_cast<int>(t / nq);
@@ -490,7 +530,7 @@ __global__ void pd_combine_terms(const double *__restrict__ pairsum,
     const double fw = ffW ? ffW[q] : 0.0;
     const bool weighted = (nv == 4);
     double AA = 0, CC = 0, BB = 0, AC = 0, AB = 0, CB = 0;
-    for (int c = 0; c < n_cls; ++c) {  // i = j terms
+    for (int c = 0; c < (add_diag ? n_cls : 0); ++c) {  // i = j terms
         const double fa = ffA[static_cast<int64_t>(cls[c].species) * nq + q];
         const double ca = ffC ? ffC[static_cast<int64_t>(cls[c].species) * nq + q] : 0.0;
         const double n = cls[c].n;
@@ -700,23 +740,23 @@ cudaError_t launch_reduce(const double *slots, const int64_t *lptr, const int64_
                           const PdPairDev *pairs, const double *qv, int32_t n_pairs, int32_t nq,
                           int32_t K, int32_t nv, int32_t n_frames, int64_t slots_per_frame,
                           const double *radius, double qmin, double dq, int residual_form,
-                          double *pairsum, cudaStream_t st) {
+                          int add_exact, double *pairsum, cudaStream_t st) {
     const int64_t total = static_cast<int64_t>(n_pairs) * nq * n_frames;
     const int grid = static_cast<int>((total + 127) / 128);
     pd_reduce_pairs<<<grid, 128, 0, st>>>(slots, lptr, lidx, pairs, qv, n_pairs, nq, K, nv,
                                           n_frames, slots_per_frame, radius, qmin, dq,
-                                          residual_form, pairsum);
+                                          residual_form, add_exact, pairsum);
     return cudaGetLastError();
 }
 
 cudaError_t launch_combine(const double *pairsum, const PdClassDev *cls, const PdPairDev *pairs,
                            int32_t n_cls, int32_t n_pairs, int32_t nq, int32_t nv,
                            int32_t n_frames, const double *ffA, const double *ffC,
-                           const double *ffW, double *terms, cudaStream_t st) {
+                           const double *ffW, int add_diag, double *terms, cudaStream_t st) {
     const int64_t total = static_cast<int64_t>(nq) * n_frames;
     const int grid = static_cast<int>((total + 127) / 128);
     pd_combine_terms<<<grid, 128, 0, st>>>(pairsum, cls, pairs, n_cls, n_pairs, nq, nv, n_frames,
-                                           ffA, ffC, ffW, terms);
+                                           ffA, ffC, ffW, add_diag, terms);
     return cudaGetLastError();
 }
 

@@ -26,11 +26,11 @@ cudaError_t launch_reduce(const double *slots, const int64_t *lptr, const int64_
                           const PdPairDev *pairs, const double *qv, int32_t n_pairs, int32_t nq,
                           int32_t K, int32_t nv, int32_t n_frames, int64_t slots_per_frame,
                           const double *radius, double qmin, double dq, int residual_form,
-                          double *pairsum, cudaStream_t st);
+                          int add_exact, double *pairsum, cudaStream_t st);
 cudaError_t launch_combine(const double *pairsum, const PdClassDev *cls, const PdPairDev *pairs,
                            int32_t n_cls, int32_t n_pairs, int32_t nq, int32_t nv,
                            int32_t n_frames, const double *ffA, const double *ffC,
-                           const double *ffW, double *terms, cudaStream_t st);
+                           const double *ffW, int add_diag, double *terms, cudaStream_t st);
 cudaError_t launch_frame_mean(const double *terms, const double *fw, int32_t n_frames, int32_t nq,
                               double *out, cudaStream_t st);
 cudaError_t launch_ffma_probe(float *out, int iters, int grid, int block, bool packed,
