@@ -215,6 +215,46 @@ int pd_measure_fp32_peak(pd_ctx *ctx, double *tflops_ffma, double *tflops_ffma2)
 /* Number of kernel launches the context has issued since creation. */
 uint64_t pd_launch_count(pd_ctx *ctx);
 
+/* ---- allocation-free solve ----
+ * No counterpart in the reference (it has no device memory to manage).
+ *
+ * Some callers cannot allocate device memory when they call in: a process
+ * whose framework owns all device memory through its own allocator or
+ * reserved pool (a cudaMalloc there fails or fragments the pool), a latency-
+ * critical serving loop where cudaMalloc/cudaFree would synchronise the
+ * device and stall every other stream, or a plug-in loaded into a host whose
+ * memory policy it does not control. For them pd_solve_noalloc runs one
+ * solve using only a fixed scratch array compiled into the library, of
+ * PD_NOALLOC_SCRATCH_BYTES bytes. It calls no cudaMalloc, cudaFree, pool or
+ * pinned-host allocation (the host planner itself uses ordinary heap memory).
+ *
+ * Inputs and outputs stay the caller's: `req` is read as HOST memory except
+ * req->xyz, which is ignored; the coordinates are xyz_dev, DEVICE memory
+ * [n_frames][N][3]; the [6][nq] result (or the frame-weighted mean) is
+ * written to out_terms_dev, DEVICE memory. The work is enqueued on `stream`
+ * (a cudaStream_t of the current device; NULL = legacy default stream) and
+ * the call returns without waiting for it.
+ *
+ * Limits and sharing:
+ *  - A request whose device layout (tables, tile list, packed atoms, tile
+ *    partial sums) needs more than PD_NOALLOC_SCRATCH_BYTES fails with
+ *    PD_EBUDGET and a message naming both sizes, before any device work.
+ *    As a guide, an FP32 solve of 40,000 atoms with solvent at nq = 500 fits;
+ *    100,000 atoms at nq = 1,000 needs about 240 MB and is refused.
+ *  - The array occupies PD_NOALLOC_SCRATCH_BYTES of memory on every GPU that
+ *    loads the library's device code, until the process exits.
+ *  - Every call shares the array, which keeps the previous call's contents;
+ *    the call overwrites or zeroes everything it reads. Calls whose device
+ *    work overlaps (two streams, or two host threads with different streams)
+ *    race on the array: serialise them on one stream.
+ *  - The first call on each device (the current one) looks up the array's
+ *    device address and the SM count; make that first call before any stream
+ *    capture on that device.
+ */
+#define PD_NOALLOC_SCRATCH_BYTES (64ull << 20)
+int pd_solve_noalloc(const pd_request *req, const double *xyz_dev, double *out_terms_dev,
+                     void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -87,7 +87,11 @@ SIGNATURES = {
     "pd_plan_inspect": (C.c_int, [_P, C.POINTER(PdRequest), _U64P, _U64P, _U64P, _U64P]),
     "pd_measure_fp32_peak": (C.c_int, [_P, _D, _D]),
     "pd_launch_count": (C.c_uint64, [_P]),
+    "pd_solve_noalloc": (C.c_int, [C.POINTER(PdRequest), C.c_void_p, C.c_void_p, C.c_void_p]),
 }
+
+# Size of the fixed device scratch behind pd_solve_noalloc.
+PD_NOALLOC_SCRATCH_BYTES = 64 << 20
 
 _lib = None
 

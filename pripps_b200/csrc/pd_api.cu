@@ -1307,3 +1307,171 @@ int pd_measure_fp32_peak(pd_ctx *ctx, double *tflops_ffma, double *tflops_ffma2)
 uint64_t pd_launch_count(pd_ctx *ctx) { return ctx ? ctx->launches.load() : 0; }
 
 }  // extern "C"
+
+// ------------------------------------------------ allocation-free solve
+// pd_solve_noalloc runs the same pipeline as a plan execution, but every
+// device array of the request (tables, tile list, packed atoms, per-warp
+// slots, partial sums) lives in one fixed array compiled into the library
+// instead of memory from cudaMalloc or a pool. It serves callers that cannot
+// allocate device memory at call time.
+namespace {
+
+// The scratch array. Host code may not use this name as a device address: on
+// the host it names a stand-in object, so the kernels get the address that
+// cudaGetSymbolAddress returns for the current device.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[PD_NOALLOC_SCRATCH_BYTES];
+
+struct NoallocDevice {
+    char *scratch = nullptr;      // device address of g_noalloc_scratch
+    std::unique_ptr<pd_ctx> ctx;  // launch bookkeeping only: no stream, no pool
+};
+std::mutex g_noalloc_mu;
+std::map<int, NoallocDevice> g_noalloc;  // per device ordinal, set up on first use
+
+int noalloc_fail(int rc, const std::string &m) {
+    std::lock_guard<std::mutex> g(g_err_mu);
+    g_err = m;
+    return rc;
+}
+
+// The host-side checks of validate_request for a request whose coordinates
+// are device memory: ids and tables are read here, the coordinates are not.
+int noalloc_validate(const pd_request *req, std::string &msg) {
+    int rc = pd::validate_request(req, true, msg);
+    if (rc) return rc;
+    for (uint64_t i = 0; i < req->n_atoms; ++i)
+        if (req->species[i] >= req->n_species) {
+            msg = "species id at atom " + std::to_string(i) + " is >= n_species";
+            return PD_EINVAL;
+        }
+    const uint64_t nt = static_cast<uint64_t>(req->n_species) * req->nq;
+    for (uint64_t i = 0; i < nt; ++i)
+        if (!std::isfinite(req->ff_atoms[i]) ||
+            (req->ff_excluded && !std::isfinite(req->ff_excluded[i]))) {
+            msg = "non-finite form-factor table entry";
+            return PD_EINVAL;
+        }
+    if (req->hyd_weights) {
+        for (uint64_t i = 0; i < req->n_atoms; ++i)
+            if (!std::isfinite(req->hyd_weights[i])) {
+                msg = "non-finite hydration weight";
+                return PD_EINVAL;
+            }
+        for (uint64_t i = 0; i < req->nq; ++i)
+            if (!std::isfinite(req->ff_water[i])) {
+                msg = "non-finite water form factor";
+                return PD_EINVAL;
+            }
+    }
+    if (req->frame_weights) {
+        const uint64_t nf = req->n_frames ? req->n_frames : 1;
+        double s = 0.0;
+        for (uint64_t f = 0; f < nf; ++f) {
+            if (!std::isfinite(req->frame_weights[f])) {
+                msg = "non-finite frame weight";
+                return PD_EINVAL;
+            }
+            s += req->frame_weights[f];
+        }
+        if (!std::isnormal(std::fabs(s))) {
+            msg = "frame weights sum to zero or a non-normal value; cannot normalize";
+            return PD_EINVAL;
+        }
+    }
+    return PD_OK;
+}
+
+// Once per device, with that device current: the scratch address and the SM
+// count. Returns the device's entry or nullptr (g_err set).
+NoallocDevice *noalloc_device(int dev, int *rc) {
+    std::lock_guard<std::mutex> g(g_noalloc_mu);
+    auto it = g_noalloc.find(dev);
+    if (it != g_noalloc.end()) return &it->second;
+    int major = 0, sms = 0;
+    cudaError_t e = cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess || major < 10) {
+        *rc = noalloc_fail(PD_ENODEV, "pd_solve_noalloc: device " + std::to_string(dev) +
+                                          " is not an sm_100 device" +
+                                          (e != cudaSuccess ? std::string(": ") +
+                                                                  cudaGetErrorString(e)
+                                                            : std::string()));
+        return nullptr;
+    }
+    void *p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+        *rc = noalloc_fail(PD_EDEVICE, std::string("pd_solve_noalloc: scratch address: ") +
+                                           cudaGetErrorString(e));
+        return nullptr;
+    }
+    NoallocDevice nd;
+    nd.scratch = static_cast<char *>(p);
+    nd.ctx = std::make_unique<pd_ctx>();
+    nd.ctx->device = dev;
+    nd.ctx->sm_count = sms;
+    return &g_noalloc.emplace(dev, std::move(nd)).first->second;
+}
+
+}  // namespace
+
+extern "C" int pd_solve_noalloc(const pd_request *req, const double *xyz_dev,
+                                double *out_terms_dev, void *stream) {
+    if (!req || !xyz_dev || !out_terms_dev)
+        return noalloc_fail(PD_EINVAL, "pd_solve_noalloc: req, xyz_dev and out_terms_dev are required");
+    pd_request r = *req;
+    r.xyz = xyz_dev;  // only checked for NULL; never read on the host
+    std::string msg;
+    int rc = noalloc_validate(&r, msg);
+    if (rc) return noalloc_fail(rc, "pd_solve_noalloc: " + msg);
+    DevPlan dp;
+    Tuning tun = tuning_for(nullptr, static_cast<int64_t>(r.n_atoms), static_cast<int64_t>(r.nq),
+                            static_cast<int>(r.precision));
+    rc = pd::build_plan(&r, r.species, r.hyd_weights, tun, dp.P, msg);
+    if (rc) return noalloc_fail(rc, "pd_solve_noalloc: " + msg);
+    dp.L = make_layout(dp.P, false);
+    if (dp.L.total > PD_NOALLOC_SCRATCH_BYTES)
+        return noalloc_fail(PD_EBUDGET,
+                            "pd_solve_noalloc: the request needs " + std::to_string(dp.L.total) +
+                                " bytes of device scratch; the fixed scratch holds " +
+                                std::to_string(static_cast<uint64_t>(PD_NOALLOC_SCRATCH_BYTES)) +
+                                " (use pd_solve or a plan for larger requests)");
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess)
+        return noalloc_fail(PD_ENODEV, std::string("pd_solve_noalloc: no current CUDA device: ") +
+                                           cudaGetErrorString(e));
+    NoallocDevice *nd = noalloc_device(dev, &rc);
+    if (!nd) return rc;
+    // One call at a time per device on the host; the device work of calls on
+    // different streams may still overlap, and then they race on the scratch.
+    std::lock_guard<std::mutex> g(g_noalloc_mu);
+    pd_ctx *ctx = nd->ctx.get();
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    // Host image of the uploaded part in ordinary heap memory: a copy from
+    // pageable memory returns once the driver has taken the bytes, so the
+    // image may go out of scope when this call returns.
+    std::vector<char> image(dp.L.upload_bytes);
+    dp.base = nd->scratch;
+    dp.stage = image.data();
+    stage_plan(ctx, dp, &r);
+    dp.stage = nullptr;
+    e = cudaMemcpyAsync(dp.base, image.data(), dp.L.upload_bytes, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) {
+        dp.xyz_dev = xyz_dev;
+        rc = run_devplan(ctx, dp, out_terms_dev, st);  // also zeroes the tile counter
+    } else {
+        rc = cuda_fail(ctx, e, "pd_solve_noalloc: upload");
+    }
+    dp.base = nullptr;  // the scratch is never freed
+    if (rc) {
+        std::string m;
+        {
+            std::lock_guard<std::mutex> g2(ctx->mu);
+            auto it = ctx->errors.find(std::this_thread::get_id());
+            if (it != ctx->errors.end()) m = it->second;
+        }
+        return noalloc_fail(rc, "pd_solve_noalloc: " + m);
+    }
+    return PD_OK;
+}
