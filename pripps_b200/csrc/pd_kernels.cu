@@ -39,81 +39,80 @@ __device__ __forceinline__ double warp_sum(double v) {
     return v;
 }
 
-// sin and cos on |h| <= π/4 as polynomials in h² whose FP32 coefficients were
-// fitted (least squares on Chebyshev nodes, each coefficient rounded to FP32
-// before the next ones were refitted): |error| < 4e-11 for sin and < 1e-11
-// for cos on the interval, in exact arithmetic, far under the FP32 rounding
-// of the result. Taylor coefficients rounded to FP32 leave a one-signed
-// error of ~1e-9, which a sum over 10^8 pairs turns into a bias.
-__device__ __forceinline__ float sin_small(float h) {
-    const float h2 = h * h;
-    float p = -2.597475088e-7f;
-    p = fmaf(p, h2, 3.148236829e-6f);
-    p = fmaf(p, h2, -1.986468124e-4f);
-    p = fmaf(p, h2, 8.333391510e-3f);
-    p = fmaf(p, h2, -1.666666716e-1f);
-    return fmaf(h * h2, p, h);
-}
-__device__ __forceinline__ float cos_small(float h) {
-    const float h2 = h * h;
-    float p = -2.870663707e-7f;
-    p = fmaf(p, h2, 2.482019954e-5f);
-    p = fmaf(p, h2, -1.388897537e-3f);
-    p = fmaf(p, h2, 4.166666791e-2f);
-    p = fmaf(p, h2, -0.5f);
-    return fmaf(h2, p, 1.0f);
+// sin and cos on |t| <= π/4 (+ a few ulp) as polynomials in t² whose FP32
+// coefficients we fitted (least squares on Chebyshev nodes, each coefficient
+// rounded to FP32 before the next ones were refitted): |error| < 8e-11 for sin
+// and < 1.1e-10 for cos in exact arithmetic, under the FP32 rounding of the
+// result and oscillating in sign. Taylor coefficients rounded to FP32 would
+// leave a one-signed error of ~1e-9, which a sum over 10^8 pairs turns into a
+// bias.
+__device__ __forceinline__ void sincos_poly(float t, float &s, float &c) {
+    const float t2 = t * t;
+    float ps = 2.789128530e-6f;
+    ps = fmaf(ps, t2, -1.984876289e-4f);
+    ps = fmaf(ps, t2, 8.333369158e-3f);
+    ps = fmaf(ps, t2, -1.666666716e-1f);
+    s = fmaf(t * t2, ps, t);
+    float pc = 2.443297126e-5f;
+    pc = fmaf(pc, t2, -1.388731296e-3f);
+    pc = fmaf(pc, t2, 4.166664556e-2f);
+    pc = fmaf(pc, t2, -0.5f);
+    c = fmaf(t2, pc, 1.0f);
 }
 
-// Three-part π/2 for the reduction: C1 has 8 significant bits, so n·C1 and
-// th − n·C1 are exact for n < 2^15; C2 = fl32(π/2 − C1); C3 = fl32(π/2 − C1 − C2).
+// Two-part π/2 for the reduction: C1 has 8 significant bits, so n·C1 and
+// a_hi − n·C1 are exact for n < 2^15; C2 = fl32(π/2 − C1). The part of π/2
+// below C2 (2.6e-12) scales every phase by the same 1 + 1.6e-12: a q-axis
+// stretch far below anything the FP64 oracle comparison can see.
 constexpr float kPio2C1 = 1.5703125f;
 constexpr float kPio2C2 = 4.838267923333e-4f;
-constexpr float kPio2C3 = 2.563282919255e-12f;
+constexpr float kRoundMagic = 12582912.0f;  // 1.5·2^23: fma(a, 2/π, magic) rounds to an integer
 
-// sin and cos of an angle given as an unevaluated sum th_hi + th_lo
-// (|th_hi| <~ 1e4, |th_lo| a few ulp of th_hi), without a branch:
-// th = n·π/2 + t, t = (th_hi − n·C1) + (th_lo − n·C2 − n·C3), then the
-// polynomials on |t| <= π/4 and the quadrant of n.
+// Reduction of an angle a = a_hi + a_lo (unevaluated sum, |a| <~ 1e4):
+// a = n·π/2 + t with |t| <= π/4 + ε; returns t and the quadrant n mod 4.
 //
-// Why the low part: th_hi lies on the FP32 grid of its binade, and th_hi − n·C1
-// is exact, so rounding (th_hi − n·π/2) to FP32 in one step gives the same
-// rounding error to every pair of that quadrant and binade — a bias of
-// ~2e-9 per sin that survives a sum over 10^7..10^10 pairs. th_lo carries
-// the pair's own rounding residue of q·r, so the final rounding of t falls
-// at a random place between grid points and averages out.
-__device__ __forceinline__ void sincos_reduced(float th_hi, float th_lo, float &s, float &c) {
-    const float n = rintf(th_hi * 0.636619772f);
-    const float t1 = fmaf(-n, kPio2C1, th_hi);  // exact
-    float u = fmaf(-n, kPio2C2, th_lo);
-    u = fmaf(-n, kPio2C3, u);
-    const float t = t1 + u;
-    const float st = sin_small(t), ct = cos_small(t);
-    const int qd = static_cast<int>(n);
-    const bool swap = (qd & 1) != 0;
-    float ss = swap ? ct : st;
-    float cc = swap ? st : ct;
-    s = (qd & 2) ? -ss : ss;
-    c = ((qd + 1) & 2) ? -cc : cc;
+// Why the low part: a_hi lies on the FP32 grid of its binade and a_hi − n·C1
+// is exact, so rounding a_hi − n·π/2 to FP32 in one step would give the same
+// rounding error to every pair of a quadrant and binade — a bias of ~2e-9 per
+// sin that survives a sum over 10^7..10^10 pairs. a_lo carries the pair's own
+// rounding residue of q·r, so the final rounding of t falls at a pair-
+// specific place between grid points and averages out.
+__device__ __forceinline__ float reduce_pio2(float a_hi, float a_lo, int &quadrant) {
+    const float nm = fmaf(a_hi, 0.636619772f, kRoundMagic);
+    const float n = nm - kRoundMagic;  // exact
+    quadrant = __float_as_int(nm) & 3;  // the low mantissa bits hold n
+    const float t1 = fmaf(-n, kPio2C1, a_hi);
+    return t1 + fmaf(-n, kPio2C2, a_lo);
+}
+
+// sin and cos of n·π/2 + t from the polynomial values at t.
+__device__ __forceinline__ void apply_quadrant(int q, float st, float ct, float &s, float &c) {
+    const bool swap = (q & 1) != 0;
+    const float a = swap ? ct : st;
+    const float b = swap ? st : ct;
+    s = (q & 2) ? -a : a;
+    c = ((q + 1) & 2) ? -b : b;
 }
 
 // Seed of one pair for a q-block. The K values s_k = sin(θ + k x), θ = q_s r,
 // x = Δq r, are produced as two interleaved sequences, even k and odd k, each
 // a sinusoid in j = k/2 with step y = 2x: s_{2j} = sin(θ + j y) and
-// s_{2j+1} = sin(θ + x + j y). With y = mπ + y' (|y'| <= π/2) and σ = (-1)^m,
-// both are σ^j·v_j where v follows the Reinsch recurrence with
-// α = 4 sin²(y'/2). Two independent chains per pair halve the dependency
-// stall of the FFMA → FADD step without adding instructions.
+// s_{2j+1} = sin(θ + x + j y). With x = m·π/2 + h (|h| <= π/4), y = mπ + 2h
+// and both sequences are σ^j·v_j, σ = (−1)^m, where v follows the Reinsch
+// recurrence with step 2h: d_{j+1} = d_j − α v_j, v_{j+1} = v_j + d_{j+1},
+// α = 4 sin²h. Two independent chains per pair halve the dependency stall of
+// the FFMA → FADD step without adding instructions.
+//
+// GENERAL_STEP = false is the path every pair of a tile takes when
+// Δq·(largest distance) <= π/4: then m = 0, h = x, σ = 1 and the step needs
+// no reduction.
 struct PairSeed {
     float ve, de, vo, dd, na, we, wo;
 };
 
-// Three-part π for the step reduction (C1 = 3.140625 has 8 significant bits).
-constexpr float kPiC1 = 3.140625f;
-constexpr float kPiC2 = 9.676535846666e-4f;
-constexpr float kPiC3 = 5.126565838511e-12f;
-
+template <bool GENERAL_STEP>
 __device__ __forceinline__ PairSeed pair_seed(float4 pi, float4 pj, bool valid, float qs_hi,
-                                              float qs_lo, float dq2_hi, float dq2_lo) {
+                                              float qs_lo, float dq_hi, float dq_lo) {
     const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
     float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
     // Coincident points: sinc(0) = 1, i.e. sin(q r)/r -> q; r = 1e-6 Å gives
@@ -125,43 +124,53 @@ __device__ __forceinline__ PairSeed pair_seed(float4 pi, float4 pj, bool valid, 
     const float r_hi = r2 * inv_r;
     const float hinv = 0.5f * inv_r;
     const float r_lo = hinv * fmaf(-r_hi, r_hi, r2);
-    // One Newton step on 1/r as well: the weight multiplies every term of the
-    // pair, so its error must be unbiased, not just small.
-    inv_r = fmaf(hinv, fmaf(-r2 * inv_r, inv_r, 1.0f), inv_r);
-    // θ = q_s·r and y = 2Δq·r as hi + lo pairs (exact product residue plus the
-    // cross terms of the two double-float factors).
+    // One Newton step on 1/r as well (1 − r2·inv² = 1 − r_hi·inv): the weight
+    // multiplies every term of the pair, so its error must be unbiased, not
+    // just small.
+    inv_r = fmaf(hinv, fmaf(-r_hi, inv_r, 1.0f), inv_r);
+    // θ = q_s·r as hi + lo (exact product residue plus the cross terms of the
+    // two double-float factors).
     const float th_hi = qs_hi * r_hi;
-    const float th_lo = fmaf(qs_hi, r_hi, -th_hi) + fmaf(qs_hi, r_lo, qs_lo * r_hi);
-    const float y_hi = dq2_hi * r_hi;
-    const float y_lo = fmaf(dq2_hi, r_hi, -y_hi) + fmaf(dq2_hi, r_lo, dq2_lo * r_hi);
-    // y = mπ + y', |y'| <= π/2, reduced like θ.
-    const float m = rintf(y_hi * 0.318309886f);
-    float yl = fmaf(-m, kPiC2, y_lo);
-    yl = fmaf(-m, kPiC3, yl);
-    const float yr = fmaf(-m, kPiC1, y_hi) + yl;
-    const int mi = static_cast<int>(m);
-    const float h = 0.5f * yr;  // x = m·π/2 + h
-    const float sh = sin_small(h), ch = cos_small(h);
-    // sin x, cos x from the quadrant of m
-    const bool swap = (mi & 1) != 0;
-    float sx = swap ? ch : sh;
-    float cx = swap ? sh : ch;
-    sx = (mi & 2) ? -sx : sx;
-    cx = ((mi + 1) & 2) ? -cx : cx;
-    float s0, c0;
-    sincos_reduced(th_hi, th_lo, s0, c0);
-    const float s1 = fmaf(s0, cx, c0 * sx);   // sin(θ + x)
-    const float c1 = fmaf(c0, cx, -s0 * sx);  // cos(θ + x)
-    const float sh2 = 2.0f * sh;
-    PairSeed ps;
-    ps.ve = s0;                                // v_0 even = sin θ
-    ps.de = sh2 * fmaf(c0, ch, s0 * sh);       // sin θ − sin(θ − y') = 2 sin h cos(θ − h)
-    ps.vo = s1;                                // v_0 odd = sin(θ + x)
-    ps.dd = sh2 * fmaf(c1, ch, s1 * sh);
-    ps.na = -sh2 * sh2;                        // −α = −4 sin² h
+    const float th_lo = fmaf(qs_lo, r_hi, fmaf(qs_hi, r_lo, fmaf(qs_hi, r_hi, -th_hi)));
+    int qt;
+    const float t = reduce_pio2(th_hi, th_lo, qt);
+    float st, ct, s0, c0;
+    sincos_poly(t, st, ct);
+    apply_quadrant(qt, st, ct, s0, c0);
     const float w = valid ? inv_r : 0.0f;
-    ps.we = w;
-    ps.wo = (mi & 1) ? -w : w;
+    PairSeed ps;
+    ps.ve = s0;  // v_0 even = sin θ
+    if (!GENERAL_STEP) {
+        // r_lo matters here: rsqrtf's error need not average to zero, and a
+        // step biased by δ moves the phase of the k-th point by k·δ.
+        const float x = fmaf(dq_hi, r_hi, fmaf(dq_hi, r_lo, dq_lo * r_hi));
+        float sx, cx;
+        sincos_poly(x, sx, cx);
+        const float sx2 = 2.0f * sx;
+        ps.de = sx2 * fmaf(c0, cx, s0 * sx);  // sin θ − sin(θ − 2x) = 2 sin x cos(θ − x)
+        ps.vo = fmaf(s0, cx, c0 * sx);        // sin(θ + x)
+        ps.dd = sx2 * c0;                     // sin(θ + x) − sin(θ − x) = 2 sin x cos θ
+        ps.na = -sx2 * sx2;                   // −α = −4 sin² x
+        ps.we = w;
+        ps.wo = w;
+    } else {
+        const float x_hi = dq_hi * r_hi;
+        const float x_lo = fmaf(dq_lo, r_hi, fmaf(dq_hi, r_lo, fmaf(dq_hi, r_hi, -x_hi)));
+        int qm;
+        const float h = reduce_pio2(x_hi, x_lo, qm);
+        float sh, ch, sx, cx;
+        sincos_poly(h, sh, ch);
+        apply_quadrant(qm, sh, ch, sx, cx);
+        const float s1 = fmaf(s0, cx, c0 * sx);   // sin(θ + x)
+        const float c1 = fmaf(c0, cx, -s0 * sx);  // cos(θ + x)
+        const float sh2 = 2.0f * sh;
+        ps.de = sh2 * fmaf(c0, ch, s0 * sh);      // sin θ − sin(θ − 2h) = 2 sin h cos(θ − h)
+        ps.vo = s1;
+        ps.dd = sh2 * fmaf(c1, ch, s1 * sh);      // sin(θ + x) − sin(θ + x − 2h)
+        ps.na = -sh2 * sh2;                       // −α = −4 sin² h
+        ps.we = w;
+        ps.wo = (qm & 1) ? -w : w;                // σ = (−1)^m
+    }
     return ps;
 }
 
@@ -175,8 +184,40 @@ __host__ __device__ __forceinline__ bool residual_q(double q, double radius) {
 }
 
 // ---------------------------------------------------------------- K1 (FP32)
-// NP pairs per thread per pass, two chains each: 2·NP independent recurrences.
-template <int K, int MODE, int NP, bool RESID>
+// Seeds of NP consecutive j atoms (clamped reads past the range are masked).
+template <int MODE, int NP, bool RESID, bool GENERAL_STEP>
+struct SeedGroup {
+    PairSeed S[NP];
+    float wj[NP];
+    float vsum, vwsum;
+
+    __device__ __forceinline__ void make(const float4 *__restrict__ at, float4 pi, int i,
+                                         bool ivalid, int j, int j1, float qs_hi, float qs_lo,
+                                         float dq_hi, float dq_lo) {
+        vsum = 0.0f;
+        vwsum = 0.0f;
+#pragma unroll
+        for (int p = 0; p < NP; ++p) {
+            const int jj = j + p;
+            const bool inr = jj < j1;
+            const float4 pj = __ldg(at + (inr ? jj : j1 - 1));
+            const bool valid = ivalid && inr && (jj > i);
+            S[p] = pair_seed<GENERAL_STEP>(pi, pj, valid, qs_hi, qs_lo, dq_hi, dq_lo);
+            if (MODE == PD_MODE_WEIGHTED) wj[p] = pj.w;
+            if (RESID) {
+                vsum += valid ? 1.0f : 0.0f;
+                if (MODE == PD_MODE_WEIGHTED) vwsum += valid ? pj.w : 0.0f;
+            }
+        }
+    }
+};
+
+// NP pairs per thread per pass, two chains each: 2·NP independent
+// recurrences. The seeds of the next pass are computed in the same straight-
+// line block as the K steps of the current one, so their long dependency
+// chains (sqrt, reductions, polynomials) overlap the recurrence instead of
+// stalling the warp between passes.
+template <int K, int MODE, int NP, bool RESID, bool GENERAL_STEP>
 __device__ __forceinline__ void pairs_range(const float4 *__restrict__ at, float4 pi, int i,
                                             bool ivalid, int j0, int j1, float qs_hi,
                                             float qs_lo, float dq_hi, float dq_lo,
@@ -184,29 +225,18 @@ __device__ __forceinline__ void pairs_range(const float4 *__restrict__ at, float
                                             float (&acc)[(MODE == PD_MODE_WEIGHTED) ? 2 : 1][K]) {
     constexpr int NACC = (MODE == PD_MODE_WEIGHTED) ? 2 : 1;
     static_assert(K % 4 == 0, "K must be a multiple of 4");
+    if (j0 >= j1) return;
+    SeedGroup<MODE, NP, RESID, GENERAL_STEP> cur;
+    cur.make(at, pi, i, ivalid, j0, j1, qs_hi, qs_lo, dq_hi, dq_lo);
     for (int j = j0; j < j1; j += NP) {
-        PairSeed S[NP];
-        float wj[NP];
-        float vsum = 0.0f, vwsum = 0.0f;
-#pragma unroll
-        for (int p = 0; p < NP; ++p) {
-            const int jj = j + p;
-            const bool inr = jj < j1;
-            const float4 pj = __ldg(at + (inr ? jj : j));
-            const bool valid = ivalid && inr && (jj > i);
-            S[p] = pair_seed(pi, pj, valid, qs_hi, qs_lo, dq_hi, dq_lo);
-            wj[p] = pj.w;
-            if (RESID) {
-                vsum += valid ? 1.0f : 0.0f;
-                if (MODE == PD_MODE_WEIGHTED) vwsum += valid ? pj.w : 0.0f;
-            }
-        }
+        SeedGroup<MODE, NP, RESID, GENERAL_STEP> nxt;  // unused after the last pass
+        nxt.make(at, pi, i, ivalid, j + NP, j1, qs_hi, qs_lo, dq_hi, dq_lo);
         float we_w[NP], wo_w[NP];
         if (MODE == PD_MODE_WEIGHTED) {
 #pragma unroll
             for (int p = 0; p < NP; ++p) {
-                we_w[p] = S[p].we * wj[p];
-                wo_w[p] = S[p].wo * wj[p];
+                we_w[p] = cur.S[p].we * cur.wj[p];
+                wo_w[p] = cur.S[p].wo * cur.wj[p];
             }
         }
         // The q table is the same in every pass; an opaque zero offset keeps
@@ -222,30 +252,80 @@ __device__ __forceinline__ void pairs_range(const float4 *__restrict__ at, float
                 const bool odd_j = (h & 2) != 0;      // j = 2t+1: weight σ·w
                 if (RESID) {
                     const float qk = s_qres[kk + qoff];
-                    acc[0][kk] = fmaf(-vsum, qk, acc[0][kk]);
+                    acc[0][kk] = fmaf(-cur.vsum, qk, acc[0][kk]);
                     if (MODE == PD_MODE_WEIGHTED)
-                        acc[NACC - 1][kk] = fmaf(-vwsum, qk, acc[NACC - 1][kk]);
+                        acc[NACC - 1][kk] = fmaf(-cur.vwsum, qk, acc[NACC - 1][kk]);
                 }
 #pragma unroll
                 for (int p = 0; p < NP; ++p) {
-                    const float w = odd_j ? S[p].wo : S[p].we;
-                    float &v = odd_chain ? S[p].vo : S[p].ve;
-                    float &d = odd_chain ? S[p].dd : S[p].de;
+                    const float w = odd_j ? cur.S[p].wo : cur.S[p].we;
+                    float &v = odd_chain ? cur.S[p].vo : cur.S[p].ve;
+                    float &d = odd_chain ? cur.S[p].dd : cur.S[p].de;
                     acc[0][kk] = fmaf(w, v, acc[0][kk]);
                     if (MODE == PD_MODE_WEIGHTED)
                         acc[NACC - 1][kk] = fmaf(odd_j ? wo_w[p] : we_w[p], v, acc[NACC - 1][kk]);
-                    d = fmaf(S[p].na, v, d);
+                    d = fmaf(cur.S[p].na, v, d);
                     v += d;
                 }
             }
         }
+        cur = nxt;
+    }
+}
+
+// Class mode on packed FP32x2 instructions (fma.rn.f32x2 / add.rn.f32x2,
+// sm_100): the even and odd chain of a pair sit in the two halves of one
+// register pair, V = (v_even, v_odd), D = (d_even, d_odd), and so do the
+// accumulators of grid points 2t and 2t+1: one step t advances both chains
+// and both accumulators with FFMA2 + FADD2 + FFMA2. The FP32 pipe does the
+// same lane work as with scalar instructions, but a warp needs half the issue
+// slots for it, which leaves the issue port to the seeds and lets the FMA
+// pipe, not instruction issue, bound the kernel. Each half rounds exactly as
+// the scalar fmaf/add would.
+template <int K, int NP, bool RESID, bool GENERAL_STEP>
+__device__ __forceinline__ void pairs_range_x2(const float4 *__restrict__ at, float4 pi, int i,
+                                               bool ivalid, int j0, int j1, float qs_hi,
+                                               float qs_lo, float dq_hi, float dq_lo,
+                                               const float2 *__restrict__ s_qres2,
+                                               float2 (&acc)[K / 2]) {
+    static_assert(K % 4 == 0, "K must be a multiple of 4");
+    if (j0 >= j1) return;
+    SeedGroup<PD_MODE_CLASS, NP, RESID, GENERAL_STEP> cur;
+    cur.make(at, pi, i, ivalid, j0, j1, qs_hi, qs_lo, dq_hi, dq_lo);
+    for (int j = j0; j < j1; j += NP) {
+        SeedGroup<PD_MODE_CLASS, NP, RESID, GENERAL_STEP> nxt;  // unused after the last pass
+        nxt.make(at, pi, i, ivalid, j + NP, j1, qs_hi, qs_lo, dq_hi, dq_lo);
+        float2 V[NP], D[NP], NA[NP], WE[NP], WO[NP];
+#pragma unroll
+        for (int p = 0; p < NP; ++p) {
+            V[p] = make_float2(cur.S[p].ve, cur.S[p].vo);
+            D[p] = make_float2(cur.S[p].de, cur.S[p].dd);
+            NA[p] = make_float2(cur.S[p].na, cur.S[p].na);
+            WE[p] = make_float2(cur.S[p].we, cur.S[p].we);
+            WO[p] = GENERAL_STEP ? make_float2(cur.S[p].wo, cur.S[p].wo) : WE[p];
+        }
+        const float2 mvs = make_float2(-cur.vsum, -cur.vsum);
+        int qoff = 0;  // opaque zero: keeps the K/2 q loads in the loop
+        if (RESID) asm volatile("mov.b32 %0, %0;" : "+r"(qoff));
+#pragma unroll
+        for (int t = 0; t < K / 2; ++t) {
+            if (RESID) acc[t] = __ffma2_rn(mvs, s_qres2[t + qoff], acc[t]);
+#pragma unroll
+            for (int p = 0; p < NP; ++p) {
+                acc[t] = __ffma2_rn((t & 1) ? WO[p] : WE[p], V[p], acc[t]);
+                D[p] = __ffma2_rn(NA[p], V[p], D[p]);
+                V[p] = __fadd2_rn(V[p], D[p]);
+            }
+        }
+        cur = nxt;
     }
 }
 
 // Resident CTAs per SM each FP32 shape is compiled for (register budget
 // 65536 / (128 · blocks) per thread).
 constexpr int fp32_min_blocks(int K, int MODE, int NP) {
-    return MODE == PD_MODE_CLASS ? (K <= 64 ? 4 : (NP == 2 ? 3 : 2)) : (K <= 32 ? 4 : 2);
+    return MODE == PD_MODE_CLASS ? (K <= 64 ? 4 : (K <= 128 && NP <= 2 ? 3 : 2))
+                                 : (K <= 32 ? 4 : 2);
 }
 
 template <int K, int MODE, int NP>
@@ -255,8 +335,9 @@ __global__ void __launch_bounds__(PD_THREADS, fp32_min_blocks(K, MODE, NP))
                                                             const PdReqDev *__restrict__ reqs,
                                                             int *__restrict__ counter) {
     constexpr int NACC = (MODE == PD_MODE_WEIGHTED) ? 2 : 1;
+    constexpr bool PACKED = (MODE == PD_MODE_CLASS);
     __shared__ int s_job;
-    __shared__ float s_qres[K];
+    __shared__ __align__(16) float s_qres[K];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const int n_jobs = *n_jobs_ptr;
@@ -270,10 +351,12 @@ __global__ void __launch_bounds__(PD_THREADS, fp32_min_blocks(K, MODE, NP))
         const int kq0 = jb.qb * K;
         const double radius = rq.radius[jb.frame];
         const bool resid = kq0 < rq.nq && residual_q(rq.qv[kq0], radius);
-        if (resid && threadIdx.x < K) {
-            const int kq = kq0 + threadIdx.x;
-            const bool on = kq < rq.nq && residual_q(rq.qv[kq], radius);
-            s_qres[threadIdx.x] = on ? static_cast<float>(rq.qv[kq]) : 0.0f;
+        if (resid) {
+            for (int t = threadIdx.x; t < K; t += PD_THREADS) {
+                const int kq = kq0 + t;
+                const bool on = kq < rq.nq && residual_q(rq.qv[kq], radius);
+                s_qres[t] = on ? static_cast<float>(rq.qv[kq]) : 0.0f;
+            }
         }
         __syncthreads();  // s_qres ready; every thread has read s_job
         const float4 *__restrict__ at = rq.atoms32 + static_cast<size_t>(jb.frame) * rq.n_pad;
@@ -283,33 +366,66 @@ __global__ void __launch_bounds__(PD_THREADS, fp32_min_blocks(K, MODE, NP))
         const double qs = rq.qmin + static_cast<double>(kq0) * rq.dq;
         const float qs_hi = static_cast<float>(qs);
         const float qs_lo = static_cast<float>(qs - static_cast<double>(qs_hi));
-        const double dq2 = 2.0 * rq.dq;  // step of the even/odd chains
-        const float dq_hi = static_cast<float>(dq2);
-        const float dq_lo = static_cast<float>(dq2 - static_cast<double>(dq_hi));
+        const float dq_hi = static_cast<float>(rq.dq);
+        const float dq_lo = static_cast<float>(rq.dq - static_cast<double>(dq_hi));
+        // Every pair distance is at most 2·radius (positions are centred):
+        // below π/4 for the step angle Δq·r the seeds skip its reduction.
+        const bool general_step = rq.dq * (2.0 * radius) > 0.78;
 
-        float acc[NACC][K];
+        if constexpr (PACKED) {
+            float2 acc[K / 2];
 #pragma unroll
-        for (int a = 0; a < NACC; ++a)
+            for (int t = 0; t < K / 2; ++t) acc[t] = make_float2(0.0f, 0.0f);
+            const float2 *q2 = reinterpret_cast<const float2 *>(s_qres);
+            if (resid) {
+                if (general_step)
+                    pairs_range_x2<K, NP, true, true>(at, pi, i, ivalid, jb.j0, jb.j1, qs_hi,
+                                                      qs_lo, dq_hi, dq_lo, q2, acc);
+                else
+                    pairs_range_x2<K, NP, true, false>(at, pi, i, ivalid, jb.j0, jb.j1, qs_hi,
+                                                       qs_lo, dq_hi, dq_lo, q2, acc);
+            } else {
+                if (general_step)
+                    pairs_range_x2<K, NP, false, true>(at, pi, i, ivalid, jb.j0, jb.j1, qs_hi,
+                                                       qs_lo, dq_hi, dq_lo, q2, acc);
+                else
+                    pairs_range_x2<K, NP, false, false>(at, pi, i, ivalid, jb.j0, jb.j1, qs_hi,
+                                                        qs_lo, dq_hi, dq_lo, q2, acc);
+            }
+            // Warp-reduce and write this warp's slot: K FP64 values.
+            double *slot = rq.slots + (jb.slot + warp) * static_cast<int64_t>(K);
 #pragma unroll
-            for (int k = 0; k < K; ++k) acc[a][k] = 0.0f;
-
-        if (resid)
-            pairs_range<K, MODE, NP, true>(at, pi, i, ivalid, jb.j0, jb.j1, qs_hi, qs_lo, dq_hi,
-                                           dq_lo, s_qres, acc);
-        else
-            pairs_range<K, MODE, NP, false>(at, pi, i, ivalid, jb.j0, jb.j1, qs_hi, qs_lo, dq_hi,
-                                            dq_lo, s_qres, acc);
-
-        // Warp-reduce and write this warp's slot: [nv][K] FP64 values.
-        double *slot = rq.slots + (jb.slot + warp) * static_cast<int64_t>(K) *
-                                      (MODE == PD_MODE_WEIGHTED ? 4 : 1);
-        if (MODE == PD_MODE_CLASS) {
-#pragma unroll
-            for (int k = 0; k < K; ++k) {
-                const float v = warp_sum(acc[0][k]);
-                if (lane == (k & 31)) slot[k] = static_cast<double>(v);
+            for (int t = 0; t < K / 2; ++t) {
+                const float v0 = warp_sum(acc[t].x);
+                const float v1 = warp_sum(acc[t].y);
+                if (lane == ((2 * t) & 31)) slot[2 * t] = static_cast<double>(v0);
+                if (lane == ((2 * t + 1) & 31)) slot[2 * t + 1] = static_cast<double>(v1);
             }
         } else {
+            float acc[NACC][K];
+#pragma unroll
+            for (int a = 0; a < NACC; ++a)
+#pragma unroll
+                for (int k = 0; k < K; ++k) acc[a][k] = 0.0f;
+
+            if (resid) {
+                if (general_step)
+                    pairs_range<K, MODE, NP, true, true>(at, pi, i, ivalid, jb.j0, jb.j1, qs_hi,
+                                                         qs_lo, dq_hi, dq_lo, s_qres, acc);
+                else
+                    pairs_range<K, MODE, NP, true, false>(at, pi, i, ivalid, jb.j0, jb.j1, qs_hi,
+                                                          qs_lo, dq_hi, dq_lo, s_qres, acc);
+            } else {
+                if (general_step)
+                    pairs_range<K, MODE, NP, false, true>(at, pi, i, ivalid, jb.j0, jb.j1, qs_hi,
+                                                          qs_lo, dq_hi, dq_lo, s_qres, acc);
+                else
+                    pairs_range<K, MODE, NP, false, false>(at, pi, i, ivalid, jb.j0, jb.j1, qs_hi,
+                                                           qs_lo, dq_hi, dq_lo, s_qres, acc);
+            }
+
+            // Warp-reduce and write this warp's slot: [4][K] FP64 values.
+            double *slot = rq.slots + (jb.slot + warp) * static_cast<int64_t>(K) * 4;
             const float wi = ivalid ? pi.w : 0.0f;
 #pragma unroll
             for (int k = 0; k < K; ++k) {
@@ -678,13 +794,13 @@ static int occupancy_fp64() {
 bool valid_shape(int precision, int mode, int K, int NP) {
     if (precision == 1) return (K == 16 || K == 32) && NP == 1;
     if (mode == PD_MODE_WEIGHTED) return (K == 32 && NP == 2) || (K == 64 && NP == 2);
-    return (K == 32 && NP == 4) || (K == 64 && (NP == 2 || NP == 4)) || (K == 96 && NP == 2) ||
-           (K == 128 && (NP == 2 || NP == 4));
+    return (K == 32 && NP == 4) || (K == 64 && NP >= 1 && NP != 3) || (K == 96 && NP == 2) ||
+           (K == 128 && NP >= 1 && NP != 3) || ((K == 160 || K == 192) && NP == 1);
 }
 
 bool valid_q_block(int precision, int K) {
     if (precision == 1) return K == 16 || K == 32;
-    return K == 32 || K == 64 || K == 96 || K == 128;
+    return K == 32 || K == 64 || K == 96 || K == 128 || K == 160 || K == 192;
 }
 
 #define PD_F32(K, M, NP)                                                                 \
@@ -700,8 +816,9 @@ cudaError_t launch_pairs(int precision, int K_, int NP_, int mode, const PdJob *
         PD_F64(16, 0) PD_F64(16, 1) PD_F64(32, 0) PD_F64(32, 1)
         return cudaErrorInvalidValue;
     }
-    PD_F32(32, 0, 4) PD_F32(64, 0, 2) PD_F32(64, 0, 4) PD_F32(96, 0, 2) PD_F32(128, 0, 2)
-    PD_F32(128, 0, 4) PD_F32(32, 1, 2) PD_F32(64, 1, 2)
+    PD_F32(32, 0, 4) PD_F32(64, 0, 1) PD_F32(64, 0, 2) PD_F32(64, 0, 4) PD_F32(96, 0, 2)
+    PD_F32(128, 0, 1) PD_F32(128, 0, 2) PD_F32(128, 0, 4) PD_F32(160, 0, 1) PD_F32(192, 0, 1)
+    PD_F32(32, 1, 2) PD_F32(64, 1, 2)
     return cudaErrorInvalidValue;
 }
 
@@ -715,8 +832,9 @@ int pairs_blocks_per_sm(int precision, int K_, int NP_, int mode) {
         PD_O64(16, 0) PD_O64(16, 1) PD_O64(32, 0) PD_O64(32, 1)
         return 0;
     }
-    PD_O32(32, 0, 4) PD_O32(64, 0, 2) PD_O32(64, 0, 4) PD_O32(96, 0, 2) PD_O32(128, 0, 2)
-    PD_O32(128, 0, 4) PD_O32(32, 1, 2) PD_O32(64, 1, 2)
+    PD_O32(32, 0, 4) PD_O32(64, 0, 1) PD_O32(64, 0, 2) PD_O32(64, 0, 4) PD_O32(96, 0, 2)
+    PD_O32(128, 0, 1) PD_O32(128, 0, 2) PD_O32(128, 0, 4) PD_O32(160, 0, 1) PD_O32(192, 0, 1)
+    PD_O32(32, 1, 2) PD_O32(64, 1, 2)
     return 0;
 }
 
