@@ -165,6 +165,42 @@ def test_fp32_vs_fp64_large_qr(gpu_ctx):
     assert np.all(err < 1e-5), err
 
 
+def test_fp32_vs_fp64_full_size_100k(gpu_ctx):
+    """The full 100,000-atom ellipsoid solve (nq = 1,000 on [0, 1]) in both
+    forms: every profile of the FP32 recurrence within 1e-5 of the plain FP64
+    kernel over the whole grid (the FP64 kernel is held to 1e-10 of the oracle
+    on the 1,000- and 10,000-atom cases; the CPU oracle needs hours here).
+    Size-independent check beside it: at q = 0 every sinc is 1, so each
+    self profile is (sum of its weights)^2 and each cross profile the product
+    of the two sums."""
+    w32 = workloads.ellipsoid_solvent_100k("fp32")
+    w64 = workloads.ellipsoid_solvent_100k("fp64")
+    t32, t64 = solve(w32.request, gpu_ctx), solve(w64.request, gpu_ctx)
+    err = term_errors(t32, t64)
+    assert np.all(err < 1e-5), err
+    req = w32.request
+    a = req.ff_atoms[req.species, 0]
+    c = req.ff_excluded[req.species, 0]
+    b = req.hyd_weights * req.ff_water[0]
+    sums = {"A": np.sum(a, dtype=np.longdouble), "C": np.sum(c, dtype=np.longdouble),
+            "B": np.sum(b, dtype=np.longdouble)}
+    exact = [sums["A"] ** 2, sums["C"] ** 2, sums["B"] ** 2, sums["A"] * sums["C"],
+             sums["A"] * sums["B"], sums["C"] * sums["B"]]
+    for t in (t32, t64):
+        for r in range(6):
+            assert abs(t[r, 0] - float(exact[r])) <= 1e-12 * abs(float(exact[r])), (r, t[r, 0])
+
+
+def test_fp32_vs_fp64_trajectory_full_size(gpu_ctx):
+    """All 256 frames of the 5,000-atom trajectory (nq = 300) in one batched
+    solve per form: the frame-weighted mean of the FP32 form within 1e-5 of
+    the FP64 form at every q."""
+    t32 = solve(workloads.trajectory_5k_256("fp32").request, gpu_ctx)
+    t64 = solve(workloads.trajectory_5k_256("fp64").request, gpu_ctx)
+    err = term_errors(t32, t64)
+    assert err[0] < 1e-5, err
+
+
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
 def test_deterministic(gpu_ctx, precision):
     w = workloads.small_globule(3000, 5, nq=97, precision=precision)
