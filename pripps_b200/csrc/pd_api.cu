@@ -102,6 +102,57 @@ Layout make_layout(const Plan &P, bool host_xyz) {
 // ---------------------------------------------------------------- context
 struct PdTicket;
 
+namespace {
+
+// Pinned host blocks in power-of-two size classes, reused across requests:
+// admitting and retiring a request then calls neither cudaHostAlloc nor
+// cudaFreeHost (which waits for the whole device). Blocks go back to the pool
+// only once no copy of theirs can be in flight.
+struct PinnedPool {
+    std::mutex mu;
+    std::map<uint64_t, std::vector<char *>> free_blocks;
+    std::vector<char *> all;
+
+    static uint64_t size_class(uint64_t bytes) {
+        uint64_t c = uint64_t{64} << 10;
+        while (c < bytes) c <<= 1;
+        return c;
+    }
+    cudaError_t get(uint64_t bytes, char **out, uint64_t *cls) {
+        const uint64_t c = size_class(bytes);
+        {
+            std::lock_guard<std::mutex> g(mu);
+            auto it = free_blocks.find(c);
+            if (it != free_blocks.end() && !it->second.empty()) {
+                *out = it->second.back();
+                it->second.pop_back();
+                *cls = c;
+                return cudaSuccess;
+            }
+        }
+        char *p = nullptr;
+        const cudaError_t e = cudaHostAlloc(reinterpret_cast<void **>(&p), c, cudaHostAllocDefault);
+        if (e != cudaSuccess) return e;
+        std::lock_guard<std::mutex> g(mu);
+        all.push_back(p);
+        *out = p;
+        *cls = c;
+        return cudaSuccess;
+    }
+    void put(char *p, uint64_t cls) {
+        std::lock_guard<std::mutex> g(mu);
+        free_blocks[cls].push_back(p);
+    }
+    void release() {
+        std::lock_guard<std::mutex> g(mu);
+        for (char *p : all) cudaFreeHost(p);
+        all.clear();
+        free_blocks.clear();
+    }
+};
+
+}  // namespace
+
 struct pd_ctx {
     int device = 0;
     int sm_count = 0;
@@ -110,6 +161,7 @@ struct pd_ctx {
     std::atomic<uint64_t> launches{0};
     cudaStream_t stream = nullptr;  // blocking solves and the request loop
     cudaMemPool_t pool = nullptr;
+    PinnedPool pinned;              // staging images of planned requests
 
     std::mutex mu;  // tuning table, per-thread errors
     std::map<std::tuple<int, int, int>, Tuning> tuning;
@@ -120,11 +172,13 @@ struct pd_ctx {
     std::mutex qmu;
     std::condition_variable qcv;
     std::condition_variable done_cv;
-    std::deque<uint64_t> pending;
+    std::deque<uint64_t> pending;                       // admission order
+    std::deque<std::shared_ptr<PdTicket>> to_plan;      // awaiting host planning
+    std::condition_variable plan_cv;
     std::map<uint64_t, std::shared_ptr<PdTicket>> tickets;
     uint64_t next_ticket = 1;
     bool stop = false;
-    std::thread worker;
+    std::thread worker, planner;
     bool worker_started = false;
 
     void set_error(const std::string &m) {
@@ -153,6 +207,7 @@ struct DevPlan {
     Layout L{};
     char *base = nullptr;   // device chunk
     char *stage = nullptr;  // pinned host image of the uploaded part
+    uint64_t stage_cls = 0; // its size class in the context's pinned pool
     uint64_t charged = 0;
     bool host_xyz = false;
     const double *xyz_dev = nullptr;  // coordinates used by pack
@@ -186,7 +241,7 @@ Tuning tuning_for(pd_ctx *ctx, int64_t n, int64_t nq, int precision) {
 
 void free_devplan(pd_ctx *ctx, DevPlan &dp, cudaStream_t st) {
     if (dp.base) cudaFreeAsync(dp.base, st);
-    if (dp.stage) cudaFreeHost(dp.stage);
+    if (dp.stage) ctx->pinned.put(dp.stage, dp.stage_cls);
     dp.base = nullptr;
     dp.stage = nullptr;
     if (dp.charged) ctx->in_use.fetch_sub(dp.charged);
@@ -283,7 +338,7 @@ int plan_device(pd_ctx *ctx, const pd_request *req, DevPlan &dp, cudaStream_t st
         ctx->set_error(std::string("device allocation failed: ") + cudaGetErrorString(e));
         return PD_ENOMEM;
     }
-    e = cudaHostAlloc(reinterpret_cast<void **>(&dp.stage), dp.L.stage_bytes, cudaHostAllocDefault);
+    e = ctx->pinned.get(dp.L.stage_bytes, &dp.stage, &dp.stage_cls);
     if (e != cudaSuccess) {
         free_devplan(ctx, dp, st);
         ctx->set_error(std::string("pinned allocation failed: ") + cudaGetErrorString(e));
@@ -404,12 +459,15 @@ struct PdTicket {
     std::vector<uint32_t> species;
     DevPlan dp;
     int status = 1;                   // 1 pending/running, 0 done, < 0 error
-    bool planned = false;
+    int plan_state = 0;               // host planning: 0 not yet, 1 done, < 0 failed (code)
+    std::string plan_err;
     bool admitted = false;
     bool canceled = false;
     bool taken = false;               // result copied out by pd_wait
     size_t next_job = 0;              // first tile not yet issued
-    bool finish_issued = false;
+    bool finish_issued = false;       // reduction (or, if cancelled, the drain) enqueued
+    bool drained_only = false;        // cancelled after admission: no reduction was run
+    uint32_t used_streams = 0;        // lane streams that ran some of its tiles
     cudaEvent_t done_ev = nullptr;
     std::vector<double> result;
     std::string err;
@@ -418,37 +476,41 @@ struct PdTicket {
 
 namespace {
 
-// Step buffers of the request loop: tiles of several requests plus the
-// descriptor array they index, uploaded from pinned memory and run by a
-// captured graph (upload, counter reset, persistent pair kernel).
-struct StepBuf {
+// One lane of a step buffer: the tiles of one kernel variant, their request
+// descriptors and the counter of the persistent kernel, uploaded from pinned
+// memory and run by a captured graph (upload, counter reset, pair kernel) on
+// the lane's own stream.
+struct Lane {
     PdJob *h_jobs = nullptr, *d_jobs = nullptr;
     PdReqDev *h_reqs = nullptr, *d_reqs = nullptr;
     int *h_n = nullptr, *d_n = nullptr;
     int *d_counter = nullptr;
-    size_t cap_jobs = 0, cap_reqs = 0;
-    cudaEvent_t ev = nullptr;
-    bool busy = false;
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev = nullptr;  // recorded after the lane's last launch
+    bool busy = false;         // ev pending: h_* may still be read by the upload
     std::map<std::tuple<int, int, int, int>, cudaGraphExec_t> graphs;  // (precision, K, NP, mode)
 };
 
+constexpr int STEP_BUFS = 2;       // steps in flight
+constexpr int STEP_LANES = 4;      // kernel variants per step
 constexpr size_t STEP_MAX_JOBS = 1 << 14;
 constexpr size_t STEP_MAX_REQS = 1024;
-constexpr double STEP_PAIRQ = 4.0e10;  // ≈ 5 ms of FP32 work per step
+constexpr double STEP_COST = 4.0e10;   // ≈ 5 ms of FP32 class-mode work per step
+constexpr double RR_QUANTUM = 1.0e9;   // work a request adds per round-robin turn
 
-void ticket_fail(pd_ctx *ctx, const std::shared_ptr<PdTicket> &t, int code, const std::string &m,
-                 cudaStream_t st) {
-    t->status = code;
-    t->err = m;
-    t->t_done = now_s();
-    if (t->dp.base || t->dp.stage) free_devplan(ctx, t->dp, st);
+// Relative cost of one pair·q of a tile (FP32 class mode = 1).
+double tile_cost(const Plan &P, const PdJob &jb) {
+    double c = static_cast<double>(PD_IBLOCK) * (jb.j1 - jb.j0) * P.tun.K;
+    if (P.precision == PD_FP64) c *= 24.0;
+    if (P.mode == PD_MODE_WEIGHTED) c *= 1.5;
+    return c;
 }
 
-int step_graph(pd_ctx *ctx, StepBuf &sb, int precision, int K, int NP, int mode,
-               cudaStream_t st, cudaGraphExec_t *out) {
+int lane_graph(pd_ctx *ctx, Lane &ln, int precision, int K, int NP, int mode,
+               cudaGraphExec_t *out) {
     auto key = std::make_tuple(precision, K, NP, mode);
-    auto it = sb.graphs.find(key);
-    if (it != sb.graphs.end()) {
+    auto it = ln.graphs.find(key);
+    if (it != ln.graphs.end()) {
         *out = it->second;
         return PD_OK;
     }
@@ -459,48 +521,115 @@ int step_graph(pd_ctx *ctx, StepBuf &sb, int precision, int K, int NP, int mode,
     dummy.mode = mode;
     const int grid = persistent_grid(ctx, dummy, 1 << 30);
     cudaGraph_t g = nullptr;
-    PD_CUDA(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-    cudaMemcpyAsync(sb.d_n, sb.h_n, sizeof(int), cudaMemcpyHostToDevice, st);
-    cudaMemcpyAsync(sb.d_reqs, sb.h_reqs, sb.cap_reqs * sizeof(PdReqDev), cudaMemcpyHostToDevice, st);
-    cudaMemcpyAsync(sb.d_jobs, sb.h_jobs, sb.cap_jobs * sizeof(PdJob), cudaMemcpyHostToDevice, st);
-    cudaMemsetAsync(sb.d_counter, 0, sizeof(int), st);
-    pd::launch_pairs(precision, K, NP, mode, sb.d_jobs, sb.d_n, sb.d_reqs, sb.d_counter, grid, st);
-    PD_CUDA(ctx, cudaStreamEndCapture(st, &g));
+    PD_CUDA(ctx, cudaStreamBeginCapture(ln.st, cudaStreamCaptureModeThreadLocal));
+    cudaMemcpyAsync(ln.d_n, ln.h_n, sizeof(int), cudaMemcpyHostToDevice, ln.st);
+    cudaMemcpyAsync(ln.d_reqs, ln.h_reqs, STEP_MAX_REQS * sizeof(PdReqDev), cudaMemcpyHostToDevice,
+                    ln.st);
+    cudaMemcpyAsync(ln.d_jobs, ln.h_jobs, STEP_MAX_JOBS * sizeof(PdJob), cudaMemcpyHostToDevice,
+                    ln.st);
+    cudaMemsetAsync(ln.d_counter, 0, sizeof(int), ln.st);
+    pd::launch_pairs(precision, K, NP, mode, ln.d_jobs, ln.d_n, ln.d_reqs, ln.d_counter, grid,
+                     ln.st);
+    PD_CUDA(ctx, cudaStreamEndCapture(ln.st, &g));
     cudaGraphExec_t ge = nullptr;
     cudaError_t e = cudaGraphInstantiate(&ge, g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaGraphInstantiate");
-    sb.graphs[key] = ge;
+    ln.graphs[key] = ge;
     *out = ge;
     return PD_OK;
 }
 
-void worker_main(pd_ctx *ctx) {
-    cudaSetDevice(ctx->device);
-    cudaStream_t st = nullptr;
-    cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
-    StepBuf sbuf[2];
-    bool init_ok = true;
-    for (auto &sb : sbuf) {
-        sb.cap_jobs = STEP_MAX_JOBS;
-        sb.cap_reqs = STEP_MAX_REQS;
-        init_ok &= cudaHostAlloc(reinterpret_cast<void **>(&sb.h_jobs), sb.cap_jobs * sizeof(PdJob), 0) == cudaSuccess;
-        init_ok &= cudaHostAlloc(reinterpret_cast<void **>(&sb.h_reqs), sb.cap_reqs * sizeof(PdReqDev), 0) == cudaSuccess;
-        init_ok &= cudaHostAlloc(reinterpret_cast<void **>(&sb.h_n), sizeof(int), 0) == cudaSuccess;
-        init_ok &= cudaMalloc(reinterpret_cast<void **>(&sb.d_jobs), sb.cap_jobs * sizeof(PdJob)) == cudaSuccess;
-        init_ok &= cudaMalloc(reinterpret_cast<void **>(&sb.d_reqs), sb.cap_reqs * sizeof(PdReqDev)) == cudaSuccess;
-        init_ok &= cudaMalloc(reinterpret_cast<void **>(&sb.d_n), sizeof(int)) == cudaSuccess;
-        init_ok &= cudaMalloc(reinterpret_cast<void **>(&sb.d_counter), sizeof(int)) == cudaSuccess;
-        init_ok &= cudaEventCreateWithFlags(&sb.ev, cudaEventDisableTiming) == cudaSuccess;
-    }
-    std::vector<std::shared_ptr<PdTicket>> active;  // admitted, in admission order
-    int cur = 0;
+// Host planning of submitted requests, in submission order, off the loop
+// thread: the loop keeps issuing steps while a large request is planned.
+void planner_main(pd_ctx *ctx) {
     for (;;) {
-        std::vector<std::shared_ptr<PdTicket>> admit_try;
+        std::shared_ptr<PdTicket> t;
         {
             std::unique_lock<std::mutex> lk(ctx->qmu);
-            if (active.empty() && ctx->pending.empty() && !ctx->stop)
-                ctx->qcv.wait_for(lk, std::chrono::milliseconds(50));
+            ctx->plan_cv.wait(lk, [&] { return ctx->stop || !ctx->to_plan.empty(); });
+            if (ctx->stop) return;
+            t = ctx->to_plan.front();
+            ctx->to_plan.pop_front();
+        }
+        int rc = PD_OK;
+        std::string m;
+        if (!t->canceled) {
+            rc = plan_host(ctx, &t->req, t->req.species, t->req.hyd_weights, true, t->dp);
+            if (rc != PD_OK) {
+                std::lock_guard<std::mutex> g(ctx->mu);
+                m = ctx->errors[std::this_thread::get_id()];
+            }
+        }
+        {
+            std::lock_guard<std::mutex> lk(ctx->qmu);
+            t->plan_err = m;
+            t->plan_state = rc == PD_OK ? 1 : rc;
+        }
+        ctx->qcv.notify_all();
+    }
+}
+
+// The device request loop. Streams: `sa` admits (device chunk from the pool,
+// upload, pack), each lane of each step buffer runs its tiles, `sf` finishes
+// (slot reduction, combine, result download). Lanes wait for the admission
+// event; a request's finish waits for the lanes that ran its tiles. Steps on
+// different buffers overlap on the GPU, so the tail of one persistent kernel
+// is filled by the next.
+void worker_main(pd_ctx *ctx) {
+    cudaSetDevice(ctx->device);
+    cudaStream_t sa = nullptr, sf = nullptr;
+    cudaEvent_t ev_admit = nullptr;
+    bool init_ok = cudaStreamCreateWithFlags(&sa, cudaStreamNonBlocking) == cudaSuccess &&
+                   cudaStreamCreateWithFlags(&sf, cudaStreamNonBlocking) == cudaSuccess &&
+                   cudaEventCreateWithFlags(&ev_admit, cudaEventDisableTiming) == cudaSuccess;
+    Lane lanes[STEP_BUFS][STEP_LANES];
+    for (auto &buf : lanes)
+        for (auto &ln : buf) {
+            if (!init_ok) break;
+            init_ok &= cudaHostAlloc(reinterpret_cast<void **>(&ln.h_jobs), STEP_MAX_JOBS * sizeof(PdJob), 0) == cudaSuccess;
+            init_ok &= cudaHostAlloc(reinterpret_cast<void **>(&ln.h_reqs), STEP_MAX_REQS * sizeof(PdReqDev), 0) == cudaSuccess;
+            init_ok &= cudaHostAlloc(reinterpret_cast<void **>(&ln.h_n), sizeof(int), 0) == cudaSuccess;
+            init_ok &= cudaMalloc(reinterpret_cast<void **>(&ln.d_jobs), STEP_MAX_JOBS * sizeof(PdJob)) == cudaSuccess;
+            init_ok &= cudaMalloc(reinterpret_cast<void **>(&ln.d_reqs), STEP_MAX_REQS * sizeof(PdReqDev)) == cudaSuccess;
+            init_ok &= cudaMalloc(reinterpret_cast<void **>(&ln.d_n), sizeof(int)) == cudaSuccess;
+            init_ok &= cudaMalloc(reinterpret_cast<void **>(&ln.d_counter), sizeof(int)) == cudaSuccess;
+            init_ok &= cudaStreamCreateWithFlags(&ln.st, cudaStreamNonBlocking) == cudaSuccess;
+            init_ok &= cudaEventCreateWithFlags(&ln.ev, cudaEventDisableTiming) == cudaSuccess;
+        }
+    auto lane_of_bit = [&](int bit) -> Lane & { return lanes[bit / STEP_LANES][bit % STEP_LANES]; };
+    auto sync_all = [&] {
+        if (sa) cudaStreamSynchronize(sa);
+        if (sf) cudaStreamSynchronize(sf);
+        for (auto &buf : lanes)
+            for (auto &ln : buf)
+                if (ln.st) cudaStreamSynchronize(ln.st);
+    };
+    auto fail = [&](const std::shared_ptr<PdTicket> &t, int code, const std::string &m) {
+        sync_all();  // nothing of the request may still be in flight when its memory returns
+        std::lock_guard<std::mutex> lk(ctx->qmu);
+        t->status = code;
+        t->err = m;
+        t->t_done = now_s();
+        if (t->dp.base || t->dp.stage) free_devplan(ctx, t->dp, sa);
+        ctx->done_cv.notify_all();
+    };
+
+    std::vector<std::shared_ptr<PdTicket>> active;  // admitted, in admission order
+    bool admit_recorded = false;
+    int cur = 0;
+    size_t rr = 0;
+    for (;;) {
+        std::vector<std::shared_ptr<PdTicket>> head;  // planned front of the queue
+        {
+            std::unique_lock<std::mutex> lk(ctx->qmu);
+            bool waiting_device = false;
+            for (auto &t : active) waiting_device |= t->finish_issued;
+            if (active.empty() && !ctx->stop) {
+                bool ready = false;
+                for (uint64_t id : ctx->pending) ready |= ctx->tickets[id]->plan_state != 0;
+                if (!ready) ctx->qcv.wait_for(lk, std::chrono::milliseconds(50));
+            }
             if (ctx->stop) break;
             // drop cancelled pending tickets
             for (auto it = ctx->pending.begin(); it != ctx->pending.end();) {
@@ -514,42 +643,46 @@ void worker_main(pd_ctx *ctx) {
                     ++it;
                 }
             }
-            for (uint64_t id : ctx->pending) admit_try.push_back(ctx->tickets[id]);
+            for (uint64_t id : ctx->pending) {
+                auto t = ctx->tickets[id];
+                if (t->plan_state == 0) break;  // FIFO: wait for its planning
+                head.push_back(t);
+            }
+            (void)waiting_device;
         }
         if (!init_ok) {
             std::lock_guard<std::mutex> lk(ctx->qmu);
-            for (auto &t : admit_try) {
+            for (auto &t : head) {
                 t->status = PD_ENOMEM;
-                t->err = "request loop could not allocate its step buffers";
+                t->err = "request loop could not allocate its streams and step buffers";
+                t->t_done = now_s();
                 ctx->pending.erase(std::find(ctx->pending.begin(), ctx->pending.end(), t->id));
             }
             ctx->done_cv.notify_all();
+            if (head.empty()) std::this_thread::sleep_for(std::chrono::milliseconds(1));
             continue;
         }
         // ---- admission in FIFO order while the budget allows
-        for (auto &t : admit_try) {
-            int rc = PD_OK;
-            if (!t->planned) {
-                rc = plan_host(ctx, &t->req, t->req.species, t->req.hyd_weights, true, t->dp);
-                t->planned = (rc == PD_OK);
-            }
-            if (rc == PD_OK) rc = plan_device(ctx, &t->req, t->dp, st, /*wait=*/true);
+        bool admitted_now = false;
+        for (auto &t : head) {
+            int rc = t->plan_state < 0 ? t->plan_state : PD_OK;
+            if (rc == PD_OK) rc = plan_device(ctx, &t->req, t->dp, sa, /*wait=*/true);
             if (rc == kBudgetWait) break;  // keep FIFO order; retry after frees
-            std::lock_guard<std::mutex> lk(ctx->qmu);
-            ctx->pending.pop_front();
+            {
+                std::lock_guard<std::mutex> lk(ctx->qmu);
+                ctx->pending.pop_front();
+            }
             if (rc != PD_OK) {
-                std::string m;
-                {
+                std::string m = t->plan_err;
+                if (m.empty()) {
                     std::lock_guard<std::mutex> g(ctx->mu);
                     m = ctx->errors[std::this_thread::get_id()];
                 }
-                ticket_fail(ctx, t, rc, m, st);
-                ctx->done_cv.notify_all();
+                fail(t, rc, m);
                 continue;
             }
-            if (pack_devplan(ctx, t->dp, st) != PD_OK) {
-                ticket_fail(ctx, t, PD_EDEVICE, "pack failed", st);
-                ctx->done_cv.notify_all();
+            if (pack_devplan(ctx, t->dp, sa) != PD_OK) {
+                fail(t, PD_EDEVICE, "pack failed");
                 continue;
             }
             // the device and the pinned image hold the inputs now
@@ -563,154 +696,186 @@ void worker_main(pd_ctx *ctx) {
             t->admitted = true;
             t->t_admit = now_s();
             active.push_back(t);
+            admitted_now = true;
         }
-        if (active.empty()) continue;
-        // ---- one step: tiles of the active requests, round-robin in chunks
-        StepBuf &sb = sbuf[cur];
-        if (sb.busy) {
-            cudaEventSynchronize(sb.ev);
-            sb.busy = false;
+        if (admitted_now) {
+            cudaEventRecord(ev_admit, sa);
+            admit_recorded = true;
         }
-        // Group by kernel variant; a step runs one variant (the oldest
-        // request's) so that one captured graph covers it.
-        std::shared_ptr<PdTicket> head;
+
+        // ---- one step: round-robin turns of RR_QUANTUM over the issuable
+        // requests (rotating start), each request's tiles into the lane of
+        // its kernel variant; up to STEP_LANES variants per step.
+        std::vector<std::shared_ptr<PdTicket>> cand;
         for (auto &t : active)
-            if (!t->canceled && t->next_job < t->dp.P.jobs.size()) {
-                head = t;
-                break;
-            }
-        std::vector<std::shared_ptr<PdTicket>> finished_now;
-        if (head) {
-            const int prec = head->dp.P.precision, K = head->dp.P.tun.K, mode = head->dp.P.mode;
-            const int NP = head->dp.P.tun.NP;
-            std::vector<std::shared_ptr<PdTicket>> members;
-            for (auto &t : active)
-                if (!t->canceled && t->next_job < t->dp.P.jobs.size() &&
-                    t->dp.P.precision == prec && t->dp.P.tun.K == K && t->dp.P.mode == mode &&
-                    t->dp.P.tun.NP == NP &&
-                    members.size() < STEP_MAX_REQS)
-                    members.push_back(t);
-            size_t nj = 0;
+            if (!t->canceled && t->next_job < t->dp.P.jobs.size()) cand.push_back(t);
+        Lane *step = lanes[cur];
+        std::tuple<int, int, int, int> lane_key[STEP_LANES];
+        std::vector<std::shared_ptr<PdTicket>> members[STEP_LANES];
+        size_t nj[STEP_LANES] = {0, 0, 0, 0};
+        int n_lanes = 0;
+        if (!cand.empty()) {
+            std::vector<int> lane_of(cand.size(), -1), slot_of(cand.size(), -1);
             double work = 0;
-            // Round-robin: every member contributes tiles in turn so that a
-            // newly admitted small request is not starved by a large one.
             bool progress = true;
-            while (progress && nj < STEP_MAX_JOBS && work < STEP_PAIRQ) {
+            const size_t start = rr % cand.size();
+            while (progress && work < STEP_COST) {
                 progress = false;
-                for (size_t m = 0; m < members.size(); ++m) {
-                    auto &t = members[m];
-                    const auto &jobs = t->dp.P.jobs;
-                    size_t take = 0;
-                    while (t->next_job < jobs.size() && nj < STEP_MAX_JOBS && take < 64) {
-                        PdJob jb = jobs[t->next_job++];
-                        jb.req = static_cast<int32_t>(m);
-                        sb.h_jobs[nj++] = jb;
-                        work += static_cast<double>(PD_IBLOCK) * (jb.j1 - jb.j0) * K;
-                        ++take;
+                for (size_t c = 0; c < cand.size() && work < STEP_COST; ++c) {
+                    const size_t ci = (start + c) % cand.size();
+                    auto &t = cand[ci];
+                    const Plan &P = t->dp.P;
+                    if (t->next_job >= P.jobs.size()) continue;
+                    if (lane_of[ci] < 0) {
+                        const auto key = std::make_tuple(P.precision, P.tun.K, P.tun.NP, P.mode);
+                        int l = 0;
+                        while (l < n_lanes && lane_key[l] != key) ++l;
+                        if (l == n_lanes) {
+                            if (n_lanes == STEP_LANES) continue;  // next step
+                            Lane &ln = step[l];
+                            if (ln.busy) {  // its previous upload may still read h_*
+                                cudaEventSynchronize(ln.ev);
+                                ln.busy = false;
+                            }
+                            lane_key[n_lanes++] = key;
+                        }
+                        if (members[l].size() >= STEP_MAX_REQS) continue;
+                        lane_of[ci] = l;
+                        slot_of[ci] = static_cast<int>(members[l].size());
+                        members[l].push_back(t);
+                    }
+                    const int l = lane_of[ci];
+                    Lane &ln = step[l];
+                    double turn = 0;
+                    while (t->next_job < P.jobs.size() && nj[l] < STEP_MAX_JOBS &&
+                           turn < RR_QUANTUM) {
+                        PdJob jb = P.jobs[t->next_job++];
+                        turn += tile_cost(P, jb);
+                        jb.req = slot_of[ci];
+                        ln.h_jobs[nj[l]++] = jb;
                         progress = true;
                     }
-                    if (work >= STEP_PAIRQ || nj >= STEP_MAX_JOBS) break;
+                    work += turn;
                 }
             }
-            for (size_t m = 0; m < members.size(); ++m) {
-                std::memcpy(&sb.h_reqs[m], members[m]->dp.hptr<char>(members[m]->dp.L.req),
-                            sizeof(PdReqDev));
-            }
-            *sb.h_n = static_cast<int>(nj);
-            cudaGraphExec_t ge = nullptr;
-            int rc = step_graph(ctx, sb, prec, K, NP, mode, st, &ge);
-            if (rc == PD_OK && cudaGraphLaunch(ge, st) == cudaSuccess) {
-                ctx->launches += 1;
-            } else {
-                std::lock_guard<std::mutex> lk(ctx->qmu);
-                for (auto &t : members) ticket_fail(ctx, t, PD_EDEVICE, "step launch failed", st);
-                ctx->done_cv.notify_all();
-            }
-            for (auto &t : members)
-                if (t->status == 1 && t->next_job >= t->dp.P.jobs.size()) finished_now.push_back(t);
+            rr = start + 1;
         }
-        // requests with no tiles at all (N = 1) finish right away
-        for (auto &t : active)
-            if (t->status == 1 && !t->finish_issued && t->dp.P.jobs.empty())
-                finished_now.push_back(t);
-        for (auto &t : finished_now) {
-            if (finish_devplan(ctx, t->dp, nullptr, st) != PD_OK) {
-                std::lock_guard<std::mutex> lk(ctx->qmu);
-                ticket_fail(ctx, t, PD_EDEVICE, "reduction launch failed", st);
-                ctx->done_cv.notify_all();
+        bool launch_failed = false;
+        for (int l = 0; l < n_lanes; ++l) {
+            Lane &ln = step[l];
+            for (size_t m = 0; m < members[l].size(); ++m)
+                std::memcpy(&ln.h_reqs[m], members[l][m]->dp.hptr<char>(members[l][m]->dp.L.req),
+                            sizeof(PdReqDev));
+            *ln.h_n = static_cast<int>(nj[l]);
+            cudaGraphExec_t ge = nullptr;
+            int rc = lane_graph(ctx, ln, std::get<0>(lane_key[l]), std::get<1>(lane_key[l]),
+                                std::get<2>(lane_key[l]), std::get<3>(lane_key[l]), &ge);
+            if (rc == PD_OK && admit_recorded) {
+                if (cudaStreamWaitEvent(ln.st, ev_admit, 0) != cudaSuccess) rc = PD_EDEVICE;
+            }
+            if (rc == PD_OK && cudaGraphLaunch(ge, ln.st) == cudaSuccess &&
+                cudaEventRecord(ln.ev, ln.st) == cudaSuccess) {
+                ctx->launches += 1;
+                ln.busy = true;
+                const uint32_t bit = 1u << (cur * STEP_LANES + l);
+                for (auto &t : members[l]) t->used_streams |= bit;
+            } else {
+                launch_failed = true;
+                for (auto &t : members[l]) fail(t, PD_EDEVICE, "step launch failed");
+            }
+        }
+        if (n_lanes) cur = (cur + 1) % STEP_BUFS;
+        (void)launch_failed;
+
+        // ---- finish requests whose tiles are all issued (or drain cancelled ones)
+        for (auto &t : active) {
+            if (t->status != 1 || t->finish_issued) continue;
+            const bool all_issued = t->next_job >= t->dp.P.jobs.size();
+            if (!all_issued && !t->canceled) continue;
+            if (admit_recorded) cudaStreamWaitEvent(sf, ev_admit, 0);
+            for (int bit = 0; bit < STEP_BUFS * STEP_LANES; ++bit)
+                if (t->used_streams & (1u << bit)) cudaStreamWaitEvent(sf, lane_of_bit(bit).ev, 0);
+            if (t->canceled) {
+                t->drained_only = true;
+            } else {
+                if (finish_devplan(ctx, t->dp, nullptr, sf) != PD_OK) {
+                    fail(t, PD_EDEVICE, "reduction launch failed");
+                    continue;
+                }
+                cudaMemcpyAsync(t->dp.hptr<double>(t->dp.L.hres), t->dp.dptr<double>(t->dp.L.out),
+                                static_cast<size_t>(6) * t->dp.P.nq * 8, cudaMemcpyDeviceToHost,
+                                sf);
+            }
+            if (cudaEventCreateWithFlags(&t->done_ev, cudaEventDisableTiming) != cudaSuccess ||
+                cudaEventRecord(t->done_ev, sf) != cudaSuccess) {
+                fail(t, PD_EDEVICE, "event record failed");
                 continue;
             }
-            cudaMemcpyAsync(t->dp.hptr<double>(t->dp.L.hres), t->dp.dptr<double>(t->dp.L.out),
-                            static_cast<size_t>(6) * t->dp.P.nq * 8, cudaMemcpyDeviceToHost, st);
-            cudaEventCreateWithFlags(&t->done_ev, cudaEventDisableTiming);
-            cudaEventRecord(t->done_ev, st);
             t->finish_issued = true;
         }
-        cudaEventRecord(sb.ev, st);
-        sb.busy = true;
-        cur ^= 1;
+
         // ---- retire finished and cancelled requests
         for (auto it = active.begin(); it != active.end();) {
             auto &t = *it;
             bool remove = false;
             if (t->status < 0) {
                 remove = true;
-            } else if (t->finish_issued && cudaEventQuery(t->done_ev) == cudaSuccess) {
-                cudaEventDestroy(t->done_ev);
-                t->done_ev = nullptr;
-                const double *res = t->dp.hptr<double>(t->dp.L.hres);
-                t->result.assign(res, res + static_cast<size_t>(6) * t->dp.P.nq);
-                free_devplan(ctx, t->dp, st);
-                std::lock_guard<std::mutex> lk(ctx->qmu);
-                t->status = 0;
-                t->t_done = now_s();
-                ctx->done_cv.notify_all();
-                remove = true;
-            } else if (t->canceled && !t->finish_issued) {
-                // tiles already issued may still run: wait for the stream
-                cudaStreamSynchronize(st);
-                free_devplan(ctx, t->dp, st);
-                std::lock_guard<std::mutex> lk(ctx->qmu);
-                t->status = PD_ECANCELED;
-                t->t_done = now_s();
-                ctx->done_cv.notify_all();
-                remove = true;
+            } else if (t->finish_issued) {
+                const cudaError_t q = cudaEventQuery(t->done_ev);
+                if (q == cudaSuccess) {
+                    cudaEventDestroy(t->done_ev);
+                    t->done_ev = nullptr;
+                    if (!t->drained_only) {
+                        const double *res = t->dp.hptr<double>(t->dp.L.hres);
+                        t->result.assign(res, res + static_cast<size_t>(6) * t->dp.P.nq);
+                    }
+                    free_devplan(ctx, t->dp, sa);
+                    std::lock_guard<std::mutex> lk(ctx->qmu);
+                    t->status = t->drained_only ? PD_ECANCELED : 0;
+                    t->t_done = now_s();
+                    ctx->done_cv.notify_all();
+                    remove = true;
+                } else if (q != cudaErrorNotReady) {
+                    fail(t, PD_EDEVICE, std::string("device error: ") + cudaGetErrorString(q));
+                    remove = true;
+                }
             }
             it = remove ? active.erase(it) : it + 1;
         }
-        // When nothing new can be issued, wait for the GPU instead of spinning.
-        bool any_issuable = false;
+
+        // ---- nothing to issue: wait briefly for a submission or the GPU
+        bool issuable = false;
         for (auto &t : active)
-            if (!t->canceled && t->next_job < t->dp.P.jobs.size()) any_issuable = true;
-        if (!any_issuable && !active.empty()) {
-            bool pending_new;
-            {
-                std::lock_guard<std::mutex> lk(ctx->qmu);
-                pending_new = !ctx->pending.empty();
-            }
-            if (!pending_new) {
-                for (auto &t : active)
-                    if (t->done_ev) {
-                        cudaEventSynchronize(t->done_ev);
-                        break;
-                    }
-            }
+            if (!t->canceled && t->next_job < t->dp.P.jobs.size()) issuable = true;
+        if (!issuable && !active.empty()) {
+            std::unique_lock<std::mutex> lk(ctx->qmu);
+            bool ready = false;
+            for (uint64_t id : ctx->pending) ready |= ctx->tickets[id]->plan_state != 0;
+            if (!ready && !ctx->stop) ctx->qcv.wait_for(lk, std::chrono::microseconds(200));
         }
     }
-    cudaStreamSynchronize(st);
-    for (auto &t : active) free_devplan(ctx, t->dp, st);
-    for (auto &sb : sbuf) {
-        for (auto &kv : sb.graphs) cudaGraphExecDestroy(kv.second);
-        cudaFreeHost(sb.h_jobs);
-        cudaFreeHost(sb.h_reqs);
-        cudaFreeHost(sb.h_n);
-        cudaFree(sb.d_jobs);
-        cudaFree(sb.d_reqs);
-        cudaFree(sb.d_n);
-        cudaFree(sb.d_counter);
-        if (sb.ev) cudaEventDestroy(sb.ev);
+    sync_all();
+    for (auto &t : active) {
+        if (t->done_ev) cudaEventDestroy(t->done_ev);
+        free_devplan(ctx, t->dp, sa);
     }
-    cudaStreamDestroy(st);
+    if (sa) cudaStreamSynchronize(sa);
+    for (auto &buf : lanes)
+        for (auto &ln : buf) {
+            for (auto &kv : ln.graphs) cudaGraphExecDestroy(kv.second);
+            if (ln.h_jobs) cudaFreeHost(ln.h_jobs);
+            if (ln.h_reqs) cudaFreeHost(ln.h_reqs);
+            if (ln.h_n) cudaFreeHost(ln.h_n);
+            if (ln.d_jobs) cudaFree(ln.d_jobs);
+            if (ln.d_reqs) cudaFree(ln.d_reqs);
+            if (ln.d_n) cudaFree(ln.d_n);
+            if (ln.d_counter) cudaFree(ln.d_counter);
+            if (ln.ev) cudaEventDestroy(ln.ev);
+            if (ln.st) cudaStreamDestroy(ln.st);
+        }
+    if (ev_admit) cudaEventDestroy(ev_admit);
+    if (sa) cudaStreamDestroy(sa);
+    if (sf) cudaStreamDestroy(sf);
 }
 
 }  // namespace
@@ -777,7 +942,11 @@ void pd_ctx_destroy(pd_ctx *ctx) {
             if (kv.second->status == 1) kv.second->canceled = true;
     }
     ctx->qcv.notify_all();
-    if (ctx->worker_started) ctx->worker.join();
+    ctx->plan_cv.notify_all();
+    if (ctx->worker_started) {
+        ctx->worker.join();
+        ctx->planner.join();
+    }
     {
         std::lock_guard<std::mutex> lk(ctx->qmu);
         for (auto &kv : ctx->tickets)
@@ -787,6 +956,7 @@ void pd_ctx_destroy(pd_ctx *ctx) {
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
     cudaStreamDestroy(ctx->stream);
+    ctx->pinned.release();
     if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
     delete ctx;
 }
@@ -1051,13 +1221,16 @@ int pd_submit(pd_ctx *ctx, const pd_request *req, uint64_t *ticket) {
         std::lock_guard<std::mutex> lk(ctx->qmu);
         if (!ctx->worker_started) {
             ctx->worker = std::thread(worker_main, ctx);
+            ctx->planner = std::thread(planner_main, ctx);
             ctx->worker_started = true;
         }
         t->id = ctx->next_ticket++;
         ctx->tickets[t->id] = t;
         ctx->pending.push_back(t->id);
+        ctx->to_plan.push_back(t);
         *ticket = t->id;
     }
+    ctx->plan_cv.notify_all();
     ctx->qcv.notify_all();
     return PD_OK;
 }
