@@ -282,13 +282,19 @@ __device__ __forceinline__ void pairs_range(const float4 *__restrict__ at, float
 // slots for it, which leaves the issue port to the seeds and lets the FMA
 // pipe, not instruction issue, bound the kernel. Each half rounds exactly as
 // the scalar fmaf/add would.
+//
+// A block runs only its first `nchunk` chunks of 16 grid points: the last
+// q-block of a grid whose length is not a multiple of K skips the steps past
+// the grid end instead of computing and discarding them. (One uniform branch
+// per chunk in a single code path measured faster on B200 than a separate
+// copy of the loop for tail blocks, which raised register spills.)
 template <int K, int NP, bool RESID, bool GENERAL_STEP>
 __device__ __forceinline__ void pairs_range_x2(const float4 *__restrict__ at, float4 pi, int i,
                                                bool ivalid, int j0, int j1, float qs_hi,
                                                float qs_lo, float dq_hi, float dq_lo,
                                                const float2 *__restrict__ s_qres2,
-                                               float2 (&acc)[K / 2]) {
-    static_assert(K % 4 == 0, "K must be a multiple of 4");
+                                               float2 (&acc)[K / 2], int nchunk) {
+    static_assert(K % 16 == 0, "K must be a multiple of 16");
     if (j0 >= j1) return;
     SeedGroup<PD_MODE_CLASS, NP, RESID, GENERAL_STEP> cur;
     cur.make(at, pi, i, ivalid, j0, j1, qs_hi, qs_lo, dq_hi, dq_lo);
@@ -309,6 +315,7 @@ __device__ __forceinline__ void pairs_range_x2(const float4 *__restrict__ at, fl
         if (RESID) asm volatile("mov.b32 %0, %0;" : "+r"(qoff));
 #pragma unroll
         for (int t = 0; t < K / 2; ++t) {
+            if ((t % 8) == 0 && t / 8 >= nchunk) break;
             if (RESID) acc[t] = __ffma2_rn(mvs, s_qres2[t + qoff], acc[t]);
 #pragma unroll
             for (int p = 0; p < NP; ++p) {
@@ -377,20 +384,28 @@ __global__ void __launch_bounds__(PD_THREADS, fp32_min_blocks(K, MODE, NP))
 #pragma unroll
             for (int t = 0; t < K / 2; ++t) acc[t] = make_float2(0.0f, 0.0f);
             const float2 *q2 = reinterpret_cast<const float2 *>(s_qres);
+            // 16-point chunks of this block that lie on the grid. The
+            // small-q residual blocks (the first of a grid) run whole: a
+            // tail check there costs the register spills it saves in steps.
+            const int nchunk = (min(K, rq.nq - kq0) + 15) >> 4;
             if (resid) {
                 if (general_step)
                     pairs_range_x2<K, NP, true, true>(at, pi, i, ivalid, jb.j0, jb.j1, qs_hi,
-                                                      qs_lo, dq_hi, dq_lo, q2, acc);
+                                                      qs_lo, dq_hi, dq_lo, q2, acc,
+                                                        K / 16);
                 else
                     pairs_range_x2<K, NP, true, false>(at, pi, i, ivalid, jb.j0, jb.j1, qs_hi,
-                                                       qs_lo, dq_hi, dq_lo, q2, acc);
+                                                       qs_lo, dq_hi, dq_lo, q2, acc,
+                                                        K / 16);
             } else {
                 if (general_step)
                     pairs_range_x2<K, NP, false, true>(at, pi, i, ivalid, jb.j0, jb.j1, qs_hi,
-                                                       qs_lo, dq_hi, dq_lo, q2, acc);
+                                                       qs_lo, dq_hi, dq_lo, q2, acc,
+                                                        nchunk);
                 else
                     pairs_range_x2<K, NP, false, false>(at, pi, i, ivalid, jb.j0, jb.j1, qs_hi,
-                                                        qs_lo, dq_hi, dq_lo, q2, acc);
+                                                        qs_lo, dq_hi, dq_lo, q2, acc,
+                                                        nchunk);
             }
             // Warp-reduce and write this warp's slot: K FP64 values.
             double *slot = rq.slots + (jb.slot + warp) * static_cast<int64_t>(K);

@@ -150,22 +150,18 @@ Tuning default_tuning(int64_t n_atoms, int64_t nq, int precision) {
     }
     // Measured on B200 (class mode): K = 128 with 2 pairs per thread is the
     // fastest shape from ~4k atoms up, K = 64 with 4 pairs below; a j chunk of
-    // about N/8 atoms balances tile count against per-tile overhead.
+    // about N/8 atoms balances tile count against per-tile overhead. The last
+    // q-block of a grid runs only the 16-point chunks that lie on it, so a
+    // long block wastes at most 15 grid points per request.
     if (n_atoms < 4000) {
         t.K = 64;
         t.NP = 4;
+    } else if (nq > 128) {
+        t.K = 128;
+        t.NP = 2;
     } else {
-        // longest block that wastes at most ~12 % of the q grid
         t.K = 64;
-        t.NP = 4;
-        for (int k : {128, 96}) {
-            const int64_t nb = (nq + k - 1) / k;
-            if (nb * k - nq <= nq / 8) {
-                t.K = k;
-                t.NP = 2;
-                break;
-            }
-        }
+        t.NP = 2;
     }
     if (nq <= 32) {
         t.K = 32;
