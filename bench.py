@@ -113,7 +113,18 @@ def cpu_sample(w, n_sample=6000, n_q=8, threads=0):
     qi = np.unique(np.linspace(0, req.nq - 1, n_q).astype(np.int64)).astype(np.uint32)
     xyz = (req.xyz[0] if req.xyz.ndim == 3 else req.xyz)[:n]
     t0 = time.perf_counter()
-    if req.ff_excluded is None and req.hyd_weights is None:
+    if w.name == "sphere_grid_solvent_10k":
+        # The reference sums the three sets apart (3 self + 3 cross sums, the
+        # union's pairs once): sample the same fraction of each set.
+        from pripps_b200.workloads import grid_solvent_sets
+        a_xyz, a_sp, ffA, c_xyz, c_kind, ffC, b_xyz, b_w, ffW = grid_solvent_sets(
+            req, w.globule.pos.shape[0])
+        f = n / req.n_atoms
+        na, nc, nb = (max(1, int(round(f * len(x)))) for x in (a_xyz, c_xyz, b_xyz))
+        n = na + nc + nb
+        O.build_model_sets(a_xyz[:na], a_sp[:na], ffA, c_xyz[:nc], c_kind[:nc], ffC,
+                           b_xyz[:nb], b_w[:nb], ffW, req.qmin, req.qmax, req.nq, qi, threads)
+    elif req.ff_excluded is None and req.hyd_weights is None:
         O.vacuum(xyz, req.species[:n], req.ff_atoms, req.qmin, req.qmax, req.nq, qi, threads)
     else:
         O.build_model(xyz, req.species[:n], req.ff_atoms, req.ff_excluded,
@@ -259,9 +270,7 @@ def run_ours(args, ws, rank, local):
     # ---- plain FP64 kernel on the same structure (bounded q grid)
     fp64 = None
     if rank == 0 and not args.no_fp64:
-        from pripps_b200 import workloads as W
-        r64 = W.globule_request(w.globule, req.qmin, req.qmax, args.fp64_nq,
-                                req.ff_excluded is not None, "fp64")
+        r64 = w.with_grid(args.fp64_nq, "fp64")
         p64 = C.c_void_p()
         c64 = r64.c_struct()
         _lib.check(lib.pd_plan_create(ctx.handle, C.byref(c64), C.byref(p64)), ctx.handle)

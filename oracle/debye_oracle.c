@@ -20,6 +20,9 @@
  *   fraser_form_factor    src/solvent/fraser.rs:48-57 (+ SingleGaussian eval
  *                         src/formfactor.rs:196)
  *   SASA shell weight     src/solvent/sasa.rs:54-59
+ *   build_model with dummies at their own positions (grid / Voronoi /
+ *   caller-supplied DummySets): src/debye.rs:83-130 with
+ *   DummySet::form_factors_at src/solvent/mod.rs:357-374
  *
  * Build with -ffp-contract=off: the reference (Rust) never contracts a*b+c
  * into an FMA except where it calls mul_add explicitly, which is restated here
@@ -129,6 +132,14 @@ typedef struct {
     const double *xyz;
     const uint32_t *species;
     const double *ff_atoms, *ff_excluded, *hyd_weights, *ff_water;
+    /* Dummy sets at their own positions (sets = 1): n_exc excluded dummies at
+     * exc_xyz with form factor row exc_kind[i] of ff_excluded; n_hyd hydration
+     * dummies at hyd_xyz, B_i = hyd_weights[i]·ff_water. With sets = 0 both
+     * sets sit at the atoms (exc_kind = species). */
+    int sets;
+    size_t n_exc, n_hyd;
+    const double *exc_xyz, *hyd_xyz;
+    const uint32_t *exc_kind;
     const double *qv;
     size_t nq;
     const uint32_t *q_index;
@@ -152,16 +163,19 @@ static long pdo_take(pdo_job *jb) {
 static void *pdo_worker(void *arg) {
     pdo_job *jb = (pdo_job *)arg;
     size_t n = jb->n;
+    size_t n_exc = jb->sets ? jb->n_exc : (jb->ff_excluded ? n : 0);
+    size_t n_hyd = jb->sets ? jb->n_hyd : (jb->hyd_weights ? n : 0);
+    const double *exc_xyz = jb->sets ? jb->exc_xyz : jb->xyz;
+    const double *hyd_xyz = jb->sets ? jb->hyd_xyz : jb->xyz;
+    const uint32_t *exc_kind = jb->sets ? jb->exc_kind : jb->species;
     double *fa = (double *)malloc(sizeof(double) * (n ? n : 1));
-    double *fc = (double *)malloc(sizeof(double) * (n ? n : 1));
-    double *fb = (double *)malloc(sizeof(double) * (n ? n : 1));
+    double *fc = (double *)malloc(sizeof(double) * (n_exc ? n_exc : 1));
+    double *fb = (double *)malloc(sizeof(double) * (n_hyd ? n_hyd : 1));
     if (!fa || !fc || !fb) {
         pthread_mutex_lock(&jb->lock);
         jb->failed = 1;
         pthread_mutex_unlock(&jb->lock);
     } else {
-        size_t n_exc = jb->ff_excluded ? n : 0;
-        size_t n_hyd = jb->hyd_weights ? n : 0;
         long t;
         while ((t = pdo_take(jb)) >= 0) {
             size_t k = jb->q_index ? jb->q_index[t] : (size_t)t;
@@ -179,18 +193,18 @@ static void *pdo_worker(void *arg) {
             }
             /* DummySet::form_factors_at (src/solvent/mod.rs:357-374) */
             for (size_t i = 0; i < n_exc; ++i)
-                fc[i] = jb->ff_excluded[(size_t)jb->species[i] * jb->nq + k];
+                fc[i] = jb->ff_excluded[(size_t)exc_kind[i] * jb->nq + k];
             if (n_hyd) {
                 double shared = jb->ff_water[k];
                 for (size_t i = 0; i < n_hyd; ++i) fb[i] = jb->hyd_weights[i] * shared;
             }
             double *o = jb->out + 6 * (size_t)t;
             o[0] = selfs(jb->xyz, fa, n, q);
-            o[1] = selfs(jb->xyz, fc, n_exc, q);
-            o[2] = selfs(jb->xyz, fb, n_hyd, q);
-            o[3] = cross(jb->xyz, fa, n, jb->xyz, fc, n_exc, q);
-            o[4] = cross(jb->xyz, fa, n, jb->xyz, fb, n_hyd, q);
-            o[5] = cross(jb->xyz, fc, n_exc, jb->xyz, fb, n_hyd, q);
+            o[1] = selfs(exc_xyz, fc, n_exc, q);
+            o[2] = selfs(hyd_xyz, fb, n_hyd, q);
+            o[3] = cross(jb->xyz, fa, n, exc_xyz, fc, n_exc, q);
+            o[4] = cross(jb->xyz, fa, n, hyd_xyz, fb, n_hyd, q);
+            o[5] = cross(exc_xyz, fc, n_exc, hyd_xyz, fb, n_hyd, q);
         }
     }
     free(fa);
@@ -255,6 +269,51 @@ int pdo_build_model(size_t n, const double *xyz, const uint32_t *species, size_t
     jb.ff_excluded = ff_excluded;
     jb.hyd_weights = hyd_weights;
     jb.ff_water = ff_water;
+    jb.qv = qv;
+    jb.nq = nq;
+    jb.q_index = q_index;
+    jb.nqi = q_index ? n_q_index : nq;
+    jb.solvent = 1;
+    jb.precise = precise;
+    jb.out = out;
+    int rc = pdo_run(&jb, n_threads);
+    free(qv);
+    return rc;
+}
+
+/*
+ * build_model with the excluded-volume and hydration dummies at their own
+ * positions (src/debye.rs:83-130): the excluded set is n_exc points exc_xyz
+ * whose form factor at q_k is ff_excluded[exc_kind[i]][k] (DummySet::PerDummy,
+ * or Weighted with weights folded into the rows); the hydration set is n_hyd
+ * points hyd_xyz with B_i(q_k) = hyd_weights[i]·ff_water[k] (DummySet::
+ * Weighted, src/solvent/mod.rs:365-371). Either set may be empty (n = 0,
+ * pointers NULL). Output as pdo_build_model.
+ */
+int pdo_build_model_sets(size_t n, const double *xyz, const uint32_t *species,
+                         const double *ff_atoms, size_t n_exc, const double *exc_xyz,
+                         const uint32_t *exc_kind, const double *ff_excluded, size_t n_hyd,
+                         const double *hyd_xyz, const double *hyd_weights,
+                         const double *ff_water, double qmin, double qmax, size_t nq,
+                         const uint32_t *q_index, size_t n_q_index, int n_threads, int precise,
+                         double *out) {
+    double *qv = (double *)malloc(sizeof(double) * (nq ? nq : 1));
+    if (!qv) return -1;
+    pdo_linear_q_values(qmin, qmax, nq, qv);
+    pdo_job jb = {0};
+    jb.n = n;
+    jb.xyz = xyz;
+    jb.species = species;
+    jb.ff_atoms = ff_atoms;
+    jb.ff_excluded = ff_excluded;
+    jb.hyd_weights = hyd_weights;
+    jb.ff_water = ff_water;
+    jb.sets = 1;
+    jb.n_exc = n_exc;
+    jb.n_hyd = n_hyd;
+    jb.exc_xyz = exc_xyz;
+    jb.hyd_xyz = hyd_xyz;
+    jb.exc_kind = exc_kind;
     jb.qv = qv;
     jb.nq = nq;
     jb.q_index = q_index;

@@ -48,6 +48,10 @@ def lib():
         L.pdo_build_model.argtypes = [C.c_size_t, _D, _U32, C.c_size_t, _D, _D, _D, _D,
                                       C.c_double, C.c_double, C.c_size_t, _U32, C.c_size_t,
                                       C.c_int, C.c_int, _D]
+        L.pdo_build_model_sets.restype = C.c_int
+        L.pdo_build_model_sets.argtypes = [C.c_size_t, _D, _U32, _D, C.c_size_t, _D, _U32, _D,
+                                           C.c_size_t, _D, _D, _D, C.c_double, C.c_double,
+                                           C.c_size_t, _U32, C.c_size_t, C.c_int, C.c_int, _D]
         L.pdo_vacuum.restype = C.c_int
         L.pdo_vacuum.argtypes = [C.c_size_t, _D, _U32, _D, C.c_double, C.c_double, C.c_size_t,
                                  _U32, C.c_size_t, C.c_int, C.c_int, _D]
@@ -110,6 +114,38 @@ def build_model(xyz, species, ff_atoms, ff_excluded=None, hyd_weights=None, ff_w
                                _d(_c(hyd_weights)), _d(_c(ff_water)), qmin, qmax, nq,
                                None if qi is None else qi.ctypes.data_as(_U32), nqi, int(threads),
                                int(bool(precise)), _d(out))
+    if rc != 0:
+        raise MemoryError("oracle allocation failed")
+    return out
+
+
+def build_model_sets(xyz, species, ff_atoms, exc_xyz=None, exc_kind=None, ff_excluded=None,
+                     hyd_xyz=None, hyd_weights=None, ff_water=None, qmin=0.0, qmax=0.5,
+                     nq=None, q_index=None, threads=0, precise=False) -> np.ndarray:
+    """[len(q_index) or nq, 6] terms of build_model with the excluded-volume
+    and hydration dummies at their own positions (src/debye.rs:83-130):
+    excluded dummy i at exc_xyz[i] has form factor ff_excluded[exc_kind[i]],
+    hydration dummy i at hyd_xyz[i] has hyd_weights[i]·ff_water."""
+    xyz = _c(xyz).reshape(-1, 3)
+    species = _c(species, np.uint32)
+    ff_atoms = _c(ff_atoms)
+    nq = ff_atoms.shape[1] if nq is None else nq
+    n_exc = 0 if exc_xyz is None else len(exc_kind)
+    n_hyd = 0 if hyd_xyz is None else len(hyd_weights)
+    exc_xyz = None if n_exc == 0 else _c(exc_xyz).reshape(-1, 3)
+    exc_kind = None if n_exc == 0 else _c(exc_kind, np.uint32)
+    hyd_xyz = None if n_hyd == 0 else _c(hyd_xyz).reshape(-1, 3)
+    hyd_w = None if n_hyd == 0 else _c(hyd_weights)
+    qi = None if q_index is None else _c(q_index, np.uint32)
+    nqi = nq if qi is None else len(qi)
+    out = np.empty((nqi, 6))
+    rc = lib().pdo_build_model_sets(
+        len(species), _d(xyz), species.ctypes.data_as(_U32), _d(ff_atoms), n_exc, _d(exc_xyz),
+        None if exc_kind is None else exc_kind.ctypes.data_as(_U32),
+        _d(None if n_exc == 0 else _c(ff_excluded)), n_hyd, _d(hyd_xyz), _d(hyd_w),
+        _d(None if n_hyd == 0 else _c(ff_water)), qmin, qmax, nq,
+        None if qi is None else qi.ctypes.data_as(_U32), nqi, int(threads), int(bool(precise)),
+        _d(out))
     if rc != 0:
         raise MemoryError("oracle allocation failed")
     return out

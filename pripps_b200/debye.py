@@ -20,9 +20,11 @@ from typing import Optional, Sequence
 import numpy as np
 
 from . import _lib
+from .dummies import DummySet
 from .errors import ValidationError
 from .formfactor import FormFactorMap, linear_q_values, read_formfactors
-from .solvent import SolventConfig, excluded_table, sasa_weights, water_table
+from .solvent import (SolventConfig, distinct_dummy_sets, excluded_table, sasa_weights,
+                      water_table)
 from .structure import Structure, structure_from_xyz
 
 TERM_NAMES = ("atoms", "excluded", "hydration", "atom_excluded", "atom_hydration",
@@ -163,15 +165,74 @@ def make_request(structure: Structure, formfactors: FormFactorMap, q_values: np.
     compact = np.searchsorted(used, ids).astype(np.uint32)
     ffA = formfactors.table(used, q_values)
     ffC = hw = ffW = None
+    exc = hyd = None
     if solvent is not None and solvent.is_active():
         ffC = excluded_table(solvent.excluded, formfactors, used, q_values,
                              solvent.bulk_electron_density)
-        if solvent.hydration.is_active():
+        if solvent.hydration.at_atoms():
             hw = sasa_weights(solvent.hydration, formfactors, ids)
             ffW = water_table(formfactors, q_values)
+        if frames is None:
+            exc, hyd = distinct_dummy_sets(solvent, structure.pos, ids, formfactors)
+        elif not (solvent.excluded.at_atoms() or solvent.excluded.kind == "disabled") or \
+                not (solvent.hydration.at_atoms() or solvent.hydration.kind == "disabled"):
+            raise ValidationError("dummies away from the atoms depend on each frame; solve "
+                                  "the frames one at a time")
     xyz = structure.pos if frames is None else np.asarray(frames, dtype=np.float64)
-    return DebyeRequest(xyz, compact, ffA, ffC, hw, ffW, qmin, qmax, len(q_values),
-                        frame_weights, precision)
+    if exc is None and hyd is None:
+        return DebyeRequest(xyz, compact, ffA, ffC, hw, ffW, qmin, qmax, len(q_values),
+                            frame_weights, precision)
+    return union_request(structure.pos, compact, ffA, ffC, hw, ffW, exc, hyd, q_values, qmin,
+                         qmax, precision)
+
+
+def union_request(pos: np.ndarray, species: np.ndarray, ffA: np.ndarray,
+                  ffC: Optional[np.ndarray], hw: Optional[np.ndarray], ffW: Optional[np.ndarray],
+                  exc: Optional[DummySet], hyd: Optional[DummySet], q_values: np.ndarray,
+                  qmin: float, qmax: float, precision: str = "fp32") -> DebyeRequest:
+    """One request over atoms, excluded-volume dummies and hydration dummies
+    as a single point set (the reference's build_model with dummies at their
+    own positions, src/debye.rs:83-130).
+
+    Species rows are extended so that each point carries only its own set's
+    factor: atoms keep their A rows (and their C rows / SASA weights when those
+    models sit at the atoms), excluded dummies get A = 0 and one C row per
+    distinct dummy form factor, hydration dummies get A = C = 0 and
+    B = w·F_water through the hydration weights. The sum over all unordered
+    pairs of the union then splits exactly into the reference's three self
+    sums (pairs within a set) and three cross sums (pairs across sets), and the
+    i = j terms of the cross profiles vanish, as they must for distinct
+    points."""
+    S, nq = ffA.shape
+    n = len(pos)
+    xyz, sp, rows_a, rows_c, wts = [pos], [np.asarray(species, dtype=np.int64)], [ffA], [], []
+    rows_c.append(ffC if ffC is not None else np.zeros((S, nq)))
+    wts.append(hw if hw is not None else np.zeros(n))
+    has_c, water = ffC is not None, ffW
+    nxt = S
+    if exc is not None and len(exc):
+        idx, rows = exc.rows(q_values)
+        xyz.append(exc.positions)
+        sp.append(nxt + idx)
+        rows_a.append(np.zeros_like(rows))
+        rows_c.append(rows)
+        wts.append(np.zeros(len(exc)))
+        nxt += rows.shape[0]
+        has_c = True
+    has_b = hw is not None
+    if hyd is not None and len(hyd):
+        xyz.append(hyd.positions)
+        sp.append(np.full(len(hyd), nxt, dtype=np.int64))
+        rows_a.append(np.zeros((1, nq)))
+        rows_c.append(np.zeros((1, nq)))
+        wts.append(hyd.weights)
+        water = np.array([hyd.form_factors[0].eval(float(q)) for q in q_values])
+        nxt += 1
+        has_b = True
+    return DebyeRequest(np.concatenate(xyz), np.concatenate(sp).astype(np.uint32),
+                        np.vstack(rows_a), np.vstack(rows_c) if has_c else None,
+                        np.concatenate(wts) if has_b else None, water if has_b else None,
+                        qmin, qmax, len(q_values), None, precision)
 
 
 def solve(req: DebyeRequest, ctx: Optional[_lib.Context] = None) -> np.ndarray:
@@ -263,6 +324,28 @@ class Pripps:
         if not np.isfinite(wsum) or wsum == 0.0 or abs(wsum) < np.finfo(float).tiny:
             raise ValidationError(
                 f"weights of the {len(w)} averaged frames sum to {wsum}; cannot normalize")
+        per_frame = active is not None and not (
+            active.excluded.kind == "disabled" or active.excluded.at_atoms()) or (
+            active is not None and not (active.hydration.kind == "disabled" or
+                                        active.hydration.at_atoms()))
+        if per_frame:
+            # Dummies away from the atoms are rebuilt from every frame
+            # (src/trajectory.rs:198-223 runs the calculator per frame): the
+            # frames go to the request loop together and their totals are
+            # averaged with the frame weights.
+            from .serving import Server
+            srv = Server(self.ctx)
+            tickets = []
+            for fr in sel:
+                sf = Structure(fr, s.ids)
+                tickets.append(srv.submit(make_request(sf, self.formfactors, q, qmin, qmax,
+                                                       active, self.precision)))
+            vs = active.excluded.effective_volume_scale()
+            cd = active.hydration.effective_contrast_density()
+            total = np.zeros(len(q))
+            for wf, t in zip(w, tickets):
+                total += wf * combine(srv.wait(t), vs, cd)
+            return Intensity(q, total / wsum, None)
         req = make_request(s, self.formfactors, q, qmin, qmax, active, self.precision,
                            frames=sel, frame_weights=w)
         terms = solve(req, self.ctx)

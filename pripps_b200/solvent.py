@@ -12,19 +12,25 @@ positions — the ones the CUDA backend's colocated form serves:
   Hydration.Sasa  B_i(q) = w_i·F_H2O(q), w_i = clamp(area_i, 0, 4π(r+p)²)·3/30
                                               (src/solvent/sasa.rs:47-70)
 
-The SASA areas come from voronota-ltr in the reference, a dependency that is
-not available here; callers supply per-atom areas (or weights) instead. The
-grid and Voronoi variants place dummies away from the atoms and are not part
-of this backend (they raise UsageError).
+Models whose dummies sit at their own positions (pripps_b200.dummies):
+
+  ExcludedVolume.Grid     grid cells inside the envelope   (src/solvent/grid_excluded.rs)
+  Hydration.Grid          grid points in a shell around it  (src/solvent/grid.rs)
+  ExcludedVolume.custom / Hydration.custom   a caller-built DummySet
+
+The SASA areas and the Voronoi models come from voronota-ltr in the
+reference, a dependency that is not available here; callers supply per-atom
+areas (or weights) for SASA, and Voronoi dummies as a custom DummySet.
 """
 from __future__ import annotations
 
 import math
-from dataclasses import dataclass
+from dataclasses import dataclass, field
 from typing import Optional
 
 import numpy as np
 
+from .dummies import DummySet, grid_excluded_dummies, grid_hydration_dummies
 from .errors import UsageError, ValidationError
 from .formfactor import FormFactorMap
 
@@ -39,8 +45,10 @@ DEFAULT_BULK_DENSITY = 0.334     # e/Å³, src/solvent/mod.rs:113-120
 # ----------------------------------------------------------- excluded volume
 @dataclass(frozen=True)
 class ExcludedVolume:
-    kind: str = "disabled"        # disabled | fraser | fraser_foxs | per_kind
+    kind: str = "disabled"        # disabled | fraser | fraser_foxs | per_kind | grid | custom
     volume_scale: float = 1.0
+    spacing: float = 1.0          # grid: cell edge (Å), src/cli.rs:98-100
+    dummy_set: Optional[DummySet] = field(default=None, compare=False)
 
     @staticmethod
     def disabled() -> "ExcludedVolume":
@@ -58,6 +66,21 @@ class ExcludedVolume:
     def per_kind(volume_scale: float = 1.0) -> "ExcludedVolume":
         return ExcludedVolume("per_kind", float(volume_scale))
 
+    @staticmethod
+    def grid(spacing: float = 1.0, volume_scale: float = 1.0) -> "ExcludedVolume":
+        """Grid cells filling the envelope (src/solvent/grid_excluded.rs)."""
+        return ExcludedVolume("grid", float(volume_scale), float(spacing))
+
+    @staticmethod
+    def custom(dummies: DummySet, volume_scale: float = 1.0) -> "ExcludedVolume":
+        """Caller-built excluded-volume dummies (unit basis; the scale is
+        applied when the six profiles are combined)."""
+        return ExcludedVolume("custom", float(volume_scale), dummy_set=dummies)
+
+    def at_atoms(self) -> bool:
+        """Whether the dummies sit at the atom positions (one per atom)."""
+        return self.kind in ("fraser", "fraser_foxs", "per_kind")
+
     def is_active(self) -> bool:
         return self.kind != "disabled"
 
@@ -67,7 +90,8 @@ class ExcludedVolume:
 
     def unit_scale(self) -> "ExcludedVolume":
         """The unit basis cached models are built on (src/solvent/mod.rs:385-403)."""
-        return self if self.kind == "disabled" else ExcludedVolume(self.kind, 1.0)
+        return self if self.kind == "disabled" else ExcludedVolume(self.kind, 1.0, self.spacing,
+                                                                    self.dummy_set)
 
 
 def fraser_form_factor(q: float, volume: float, rho: float, denominator: float) -> float:
@@ -85,7 +109,7 @@ def excluded_table(cfg: ExcludedVolume, formfactors: FormFactorMap, species: np.
     six terms are combined, as the reference builds its dummies through
     unit_scale_dummies for both the cached and the one-shot Debye path
     (src/debye.rs:62-66, :83-87)."""
-    if cfg.kind == "disabled":
+    if cfg.kind == "disabled" or not cfg.at_atoms():
         return None
     out = np.empty((len(species), len(q_values)), dtype=np.float64)
     if cfg.kind in ("fraser", "fraser_foxs"):
@@ -116,11 +140,14 @@ def excluded_table(cfg: ExcludedVolume, formfactors: FormFactorMap, species: np.
 # ----------------------------------------------------------------- hydration
 @dataclass(frozen=True)
 class Hydration:
-    kind: str = "disabled"            # disabled | sasa
+    kind: str = "disabled"            # disabled | sasa | grid | custom
     probe: float = 1.8
     contrast_density: float = 0.0
     areas: Optional[tuple] = None     # per-atom SAS areas (Å²), or
     weights: Optional[tuple] = None   # per-atom shell weights directly
+    spacing: float = 3.10516          # grid: point spacing (Å), src/cli.rs:112-116
+    thickness: float = 3.0            # grid: shell thickness (Å), src/cli.rs:117-119
+    dummy_set: Optional[DummySet] = field(default=None, compare=False)
 
     @staticmethod
     def disabled() -> "Hydration":
@@ -132,6 +159,21 @@ class Hydration:
         return Hydration("sasa", float(probe), float(contrast_density),
                          None if areas is None else tuple(np.asarray(areas, dtype=float)),
                          None if weights is None else tuple(np.asarray(weights, dtype=float)))
+
+    @staticmethod
+    def grid(contrast_density: float = 0.03, spacing: float = 3.10516, thickness: float = 3.0,
+             probe: float = 1.8) -> "Hydration":
+        """Grid points in a shell around the envelope (src/solvent/grid.rs)."""
+        return Hydration("grid", float(probe), float(contrast_density), spacing=float(spacing),
+                         thickness=float(thickness))
+
+    @staticmethod
+    def custom(dummies: DummySet, contrast_density: float = 0.03) -> "Hydration":
+        """Caller-built hydration dummies (e.g. a Voronoi shell)."""
+        return Hydration("custom", 0.0, float(contrast_density), dummy_set=dummies)
+
+    def at_atoms(self) -> bool:
+        return self.kind == "sasa"
 
     def is_active(self) -> bool:
         return self.kind != "disabled"
@@ -192,3 +234,24 @@ class SolventConfig:
     def is_active(self) -> bool:
         """src/solvent/mod.rs:123-128"""
         return self.excluded.is_active() or self.hydration.is_active()
+
+
+def distinct_dummy_sets(cfg: "SolventConfig", pos: np.ndarray, ids: np.ndarray,
+                        formfactors: FormFactorMap):
+    """(excluded DummySet or None, hydration DummySet or None) for the models
+    whose dummies sit at their own positions; both None for colocated models
+    (src/solvent/mod.rs:405-470, unit basis)."""
+    exc = hyd = None
+    e, h = cfg.excluded, cfg.hydration
+    if e.kind == "grid":
+        exc = grid_excluded_dummies(pos, ids, formfactors, cfg.bulk_electron_density, e.spacing)
+    elif e.kind == "custom":
+        exc = e.dummy_set
+    if h.kind == "grid":
+        hyd = grid_hydration_dummies(pos, ids, formfactors, h.spacing, h.thickness, h.probe)
+    elif h.kind == "custom":
+        hyd = h.dummy_set
+    if hyd is not None and hyd.weights is None:
+        raise UsageError("hydration dummies must be a weighted DummySet (one shared form "
+                         "factor, per-dummy weights)")
+    return exc, hyd

@@ -74,6 +74,15 @@ class Workload:
     request: DebyeRequest
     globule: synth.Globule
 
+    def with_grid(self, nq: int, precision: str) -> DebyeRequest:
+        """The same structure and solvent model on another q grid (same
+        range) and precision form."""
+        r = self.request
+        if self.name == "sphere_grid_solvent_10k":
+            return grid_solvent_request(self.globule, r.qmin, r.qmax, nq, precision)
+        return globule_request(self.globule, r.qmin, r.qmax, nq, r.ff_excluded is not None,
+                               precision)
+
     @property
     def pairs(self) -> int:
         n = self.request.n_atoms
@@ -121,6 +130,47 @@ def trajectory_5k_256(precision="fp32", n_frames: int = 256) -> Workload:
                     globule_request(g, 0.0, 0.5, 300, False, precision, frames, w), g)
 
 
+def grid_solvent_request(g: synth.Globule, qmin: float, qmax: float, nq: int,
+                         precision: str = "fp32", excluded_spacing: float = 1.0,
+                         hydration_spacing: float = 3.10516):
+    """Atoms plus grid solvent dummies at their own positions: excluded-volume
+    cells of `excluded_spacing` Å filling the envelope (FoXS radii) and
+    hydration points of `hydration_spacing` Å in the 1.8-4.8 Å shell around it,
+    as one union request (see pripps_b200.debye.union_request)."""
+    from .debye import make_request
+    from .solvent import ExcludedVolume, Hydration, SolventConfig
+    from .structure import Structure
+    cfg = SolventConfig(ExcludedVolume.grid(excluded_spacing),
+                        Hydration.grid(0.03, spacing=hydration_spacing))
+    q = linear_q_values(qmin, qmax, nq)
+    s = Structure(g.pos, element_ids()[g.elements])
+    return make_request(s, foxs(), q, qmin, qmax, cfg, precision)
+
+
+def grid_solvent_sets(req: DebyeRequest, n_atoms: int):
+    """Split a union request (atoms first, then excluded-volume dummies, then
+    hydration dummies) back into the three sets, as the oracle's
+    build_model_sets takes them: (atoms xyz, species, ffA, excluded xyz,
+    excluded rows, ffC, hydration xyz, hydration weights, F_water)."""
+    S_atoms = int(req.species[:n_atoms].max()) + 1
+    sp = req.species.astype(np.int64)
+    exc = (sp >= S_atoms) & (req.hyd_weights == 0)
+    hyd = req.hyd_weights > 0
+    hyd[:n_atoms] = False
+    exc[:n_atoms] = False
+    return (req.xyz[:n_atoms], req.species[:n_atoms], req.ff_atoms[:S_atoms],
+            req.xyz[exc], sp[exc], req.ff_excluded, req.xyz[hyd], req.hyd_weights[hyd],
+            req.ff_water)
+
+
+def sphere_grid_solvent_10k(precision="fp32") -> Workload:
+    """The 10,000-atom sphere with grid excluded volume (1 Å cells) and a
+    grid hydration shell: ~111,000 points, nq = 500 on [0, 0.5]."""
+    g = _globule(10_000, (35.0, 35.0, 35.0), 1)
+    return Workload("sphere_grid_solvent_10k", grid_solvent_request(g, 0.0, 0.5, 500, precision),
+                    g)
+
+
 def stream_request(sr: synth.StreamRequest, precision="fp32") -> Workload:
     r = synth.sphere_radius_for(sr.n_atoms)
     g = synth.globule(sr.n_atoms, (r, r, r), sr.seed)
@@ -136,6 +186,7 @@ def small_globule(n: int, seed: int, nq: int = 40, qmax: float = 0.5, solvent: b
 
 
 WORKLOADS = {
+    "sphere_grid_solvent_10k": sphere_grid_solvent_10k,
     "sphere_vacuum_1k": sphere_vacuum_1k,
     "sphere_solvent_10k": sphere_solvent_10k,
     "ellipsoid_solvent_100k": ellipsoid_solvent_100k,
