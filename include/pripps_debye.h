@@ -41,7 +41,7 @@
 extern "C" {
 #endif
 
-#define PD_ABI_VERSION 1
+#define PD_ABI_VERSION 2
 
 /* ---- status codes ---- */
 #define PD_OK 0
@@ -62,6 +62,34 @@ extern "C" {
 #define PD_NUM_TERMS 6 /* rows of the [6][nq] output, see above */
 
 typedef struct pd_ctx pd_ctx;
+
+/*
+ * A lattice set (ABI version 2). Every point of species `species` sits at
+ * origin + spacing·(i, j, k) with integers 0 <= i < extent[0],
+ * 0 <= j < extent[1], 0 <= k < extent[2], as the reference's grid solvent
+ * models place their dummies (ExcludedVolume::Grid,
+ * src/solvent/grid_excluded.rs:34-73; Hydration::Grid, src/solvent/grid.rs:
+ * 40-95). The self pair sum of such a set depends only on the integer squared
+ * offsets n = |(i,j,k) - (i',j',k')|², so the library counts the pairs of
+ * every n exactly (integer work on the device) and evaluates
+ * Σ_n count(n)·sinc(q·spacing·√n) in FP64 instead of summing a sinc per pair:
+ * on a lattice whole classes of pairs share one distance, and a per-pair FP32
+ * evaluation would repeat the same rounding for all of them. Pairs between
+ * the set and other points are summed per pair as usual.
+ * Requirements: the species' points share one hydration weight (or there are
+ * no hydration weights), the request has one frame and fewer than 49
+ * (species, weight) classes. A point of the species that lies off the lattice
+ * by more than 1e-6·spacing or outside the extents makes the result NaN
+ * (pd_solve and pd_wait then return PD_EINVAL).
+ */
+typedef struct pd_lattice {
+    uint32_t species;    /* species id whose points form the lattice set */
+    uint32_t reserved;   /* must be 0 */
+    double origin[3];    /* Å */
+    double spacing;      /* Å, > 0 */
+    uint32_t extent[3];  /* grid steps per axis, each >= 1 */
+    uint32_t reserved2;  /* must be 0 */
+} pd_lattice;
 
 /*
  * One Debye solve. Replaces the inputs the reference's build_model gathers
@@ -87,7 +115,8 @@ typedef struct pd_request {
     uint64_t n_frames;          /* 0 or 1: one structure; > 1: trajectory batch */
     const double *frame_weights;/* [n_frames] weights of the mean, or NULL: uniform */
     uint32_t flags;             /* reserved, must be 0 */
-    uint32_t reserved;          /* must be 0 */
+    uint32_t n_lattices;        /* 0..8 lattice sets (ABI version 1: must be 0) */
+    const pd_lattice *lattices; /* [n_lattices], read only when n_lattices > 0 */
 } pd_request;
 
 /* Create a context on CUDA device `device`. `mem_budget_bytes` caps the

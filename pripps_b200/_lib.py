@@ -31,6 +31,17 @@ PD_FP64 = 1
 PRECISIONS = {"fp32": PD_FP32_FP64RED, "fp64": PD_FP64}
 
 
+class PdLattice(C.Structure):
+    _fields_ = [
+        ("species", C.c_uint32),
+        ("reserved", C.c_uint32),
+        ("origin", C.c_double * 3),
+        ("spacing", C.c_double),
+        ("extent", C.c_uint32 * 3),
+        ("reserved2", C.c_uint32),
+    ]
+
+
 class PdRequest(C.Structure):
     _fields_ = [
         ("n_atoms", C.c_uint64),
@@ -48,7 +59,8 @@ class PdRequest(C.Structure):
         ("n_frames", C.c_uint64),
         ("frame_weights", C.POINTER(C.c_double)),
         ("flags", C.c_uint32),
-        ("reserved", C.c_uint32),
+        ("n_lattices", C.c_uint32),
+        ("lattices", C.POINTER(PdLattice)),
     ]
 
 

@@ -48,11 +48,12 @@ inline uint64_t align_up(uint64_t v, uint64_t a) { return (v + a - 1) / a * a; }
 // copy; the rest is device-only scratch.
 struct Layout {
     uint64_t qv, ffA, ffC, ffW, hw, fw, cls, pairs, perm, gvalid, jobs, lptr, lidx, req, njobs,
-        xyz;
+        xyz, lat, lat_tiles;
     uint64_t upload_bytes;
     uint64_t hres;         // host-only: pinned landing area of the [6][nq] result
     uint64_t stage_bytes;  // pinned image size (upload + result area)
     uint64_t centroid, radius, atoms, slots, pairsum, terms, out, counter;
+    uint64_t lat_idx, hist, lat_err;  // lattice sets: coordinates, pair counts, error flag
     uint64_t total;
 };
 
@@ -81,6 +82,8 @@ Layout make_layout(const Plan &P, bool host_xyz) {
     L.req = take(sizeof(PdReqDev));
     L.njobs = take(sizeof(int));
     L.xyz = take(host_xyz ? static_cast<uint64_t>(P.n_atoms) * 3 * P.n_frames * 8 : 0);
+    L.lat = take(P.lat.size() * sizeof(PdLatDev));
+    L.lat_tiles = take(P.lat_tiles.size() * sizeof(PdLatTile));
     L.upload_bytes = o;
     L.hres = o;
     L.stage_bytes = align_up(o + 6 * nq * 8, 256);
@@ -93,6 +96,9 @@ Layout make_layout(const Plan &P, bool host_xyz) {
     L.terms = take(static_cast<uint64_t>(P.n_frames) * 6 * nq * 8);
     L.out = take(6 * nq * 8);
     L.counter = take(sizeof(int) * 4);
+    L.lat_idx = take(P.lat.empty() ? 0 : static_cast<uint64_t>(P.n_pad) * sizeof(int4));
+    L.hist = take(static_cast<uint64_t>(P.lat_bins) * 8);
+    L.lat_err = take(sizeof(int));
     L.total = o;
     return L;
 }
@@ -248,6 +254,18 @@ void free_devplan(pd_ctx *ctx, DevPlan &dp, cudaStream_t st) {
     dp.charged = 0;
 }
 
+// A request with lattice sets whose result came back NaN had a point off its
+// lattice (the device flags it that way; see pd_lattice in pripps_debye.h).
+bool lattice_failed(const Plan &P, const double *terms) {
+    if (P.lat.empty()) return false;
+    for (size_t i = 0; i < static_cast<size_t>(6) * P.nq; ++i)
+        if (std::isnan(terms[i])) return true;
+    return false;
+}
+constexpr const char *kLatticeMsg =
+    "a point of a lattice species lies off its lattice (by more than 1e-6 spacing) or outside "
+    "its extents";
+
 // Fill the pinned staging image (tables, layout, tiles, lists, descriptor).
 int stage_plan(pd_ctx *ctx, DevPlan &dp, const pd_request *req) {
     const Plan &P = dp.P;
@@ -269,6 +287,11 @@ int stage_plan(pd_ctx *ctx, DevPlan &dp, const pd_request *req) {
     std::memcpy(dp.hptr<char>(L.jobs), P.jobs.data(), P.jobs.size() * sizeof(PdJob));
     std::memcpy(dp.hptr<char>(L.lptr), P.lptr.data(), P.lptr.size() * 8);
     std::memcpy(dp.hptr<char>(L.lidx), P.lidx.data(), P.lidx.size() * 8);
+    if (!P.lat.empty()) {
+        std::memcpy(dp.hptr<char>(L.lat), P.lat.data(), P.lat.size() * sizeof(PdLatDev));
+        std::memcpy(dp.hptr<char>(L.lat_tiles), P.lat_tiles.data(),
+                    P.lat_tiles.size() * sizeof(PdLatTile));
+    }
     PdReqDev rd{};
     if (P.precision == PD_FP64)
         rd.atoms64 = dp.dptr<double4>(L.atoms);
@@ -372,6 +395,14 @@ int finish_devplan(pd_ctx *ctx, DevPlan &dp, double *out_dev, cudaStream_t st) {
                                    P.n_frames, P.slots_per_frame, dp.dptr<double>(L.radius),
                                    P.qmin, P.dq, P.precision == PD_FP32_FP64RED ? 1 : 0,
                                    dp.rank == 0 ? 1 : 0, dp.dptr<double>(L.pairsum), st));
+    if (!P.lat.empty()) {
+        PD_CUDA(ctx, pd::launch_lattice_sums(
+                         reinterpret_cast<const unsigned long long *>(dp.dptr<char>(L.hist)),
+                         dp.dptr<PdLatDev>(L.lat), static_cast<int>(P.lat.size()),
+                         dp.dptr<double>(L.qv), P.nq, dp.rank == 0 ? 1 : 0,
+                         dp.dptr<int>(L.lat_err), dp.dptr<double>(L.pairsum), st));
+        ctx->launches += 1;
+    }
     PD_CUDA(ctx, pd::launch_combine(dp.dptr<double>(L.pairsum), dp.dptr<PdClassDev>(L.cls),
                                     dp.dptr<PdPairDev>(L.pairs), P.n_cls, P.n_pairs, P.nq, P.nv,
                                     P.n_frames, dp.dptr<double>(L.ffA),
@@ -404,6 +435,17 @@ int pack_devplan(pd_ctx *ctx, DevPlan &dp, cudaStream_t st) {
                                  P.precision == PD_FP64 ? nullptr : dp.dptr<float4>(L.atoms),
                                  P.precision == PD_FP64 ? dp.dptr<double4>(L.atoms) : nullptr, st));
     ctx->launches += 2;
+    if (!P.lat.empty()) {
+        PD_CUDA(ctx, pd::launch_lattice(dp.xyz_dev, dp.dptr<int32_t>(L.perm),
+                                        dp.dptr<PdLatDev>(L.lat), P.lat.data(),
+                                        static_cast<int>(P.lat.size()),
+                                        dp.dptr<PdLatTile>(L.lat_tiles),
+                                        static_cast<int64_t>(P.lat_tiles.size()),
+                                        dp.dptr<int4>(L.lat_idx),
+                                        reinterpret_cast<unsigned long long *>(dp.dptr<char>(L.hist)),
+                                        P.lat_bins, dp.dptr<int>(L.lat_err), st));
+        ctx->launches += P.lat_tiles.empty() ? 1 : 2;
+    }
     return PD_OK;
 }
 
@@ -457,6 +499,7 @@ struct PdTicket {
     pd_request req{};                 // pointers below own the copies
     std::vector<double> xyz, ffA, ffC, hw, ffW, fw;
     std::vector<uint32_t> species;
+    std::vector<pd_lattice> lats;
     DevPlan dp;
     int status = 1;                   // 1 pending/running, 0 done, < 0 error
     int plan_state = 0;               // host planning: 0 not yet, 1 done, < 0 failed (code)
@@ -825,13 +868,16 @@ void worker_main(pd_ctx *ctx) {
                 if (q == cudaSuccess) {
                     cudaEventDestroy(t->done_ev);
                     t->done_ev = nullptr;
+                    bool bad_lattice = false;
                     if (!t->drained_only) {
                         const double *res = t->dp.hptr<double>(t->dp.L.hres);
                         t->result.assign(res, res + static_cast<size_t>(6) * t->dp.P.nq);
+                        bad_lattice = lattice_failed(t->dp.P, res);
                     }
                     free_devplan(ctx, t->dp, sa);
                     std::lock_guard<std::mutex> lk(ctx->qmu);
-                    t->status = t->drained_only ? PD_ECANCELED : 0;
+                    t->status = t->drained_only ? PD_ECANCELED : (bad_lattice ? PD_EINVAL : 0);
+                    if (bad_lattice) t->err = kLatticeMsg;
                     t->t_done = now_s();
                     ctx->done_cv.notify_all();
                     remove = true;
@@ -994,6 +1040,10 @@ int pd_solve(pd_ctx *ctx, const pd_request *req, double *out_terms) {
                                         cudaMemcpyDeviceToHost, ctx->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
         if (e != cudaSuccess) rc = cuda_fail(ctx, e, "pd_solve");
+        if (rc == PD_OK && lattice_failed(dp.P, out_terms)) {
+            ctx->set_error(kLatticeMsg);
+            rc = PD_EINVAL;
+        }
     }
     free_devplan(ctx, dp, ctx->stream);
     cudaStreamSynchronize(ctx->stream);
@@ -1101,6 +1151,10 @@ int pd_plan_execute_host(pd_ctx *ctx, pd_plan *plan, const double *xyz_host, dou
                                         cudaMemcpyDeviceToHost, ctx->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
         if (e != cudaSuccess) rc = cuda_fail(ctx, e, "pd_plan_execute_host");
+        if (rc == PD_OK && lattice_failed(P, out_terms)) {
+            ctx->set_error(kLatticeMsg);
+            rc = PD_EINVAL;
+        }
     }
     cudaFreeAsync(xyz_dev, ctx->stream);
     cudaStreamSynchronize(ctx->stream);
@@ -1208,7 +1262,9 @@ int pd_submit(pd_ctx *ctx, const pd_request *req, uint64_t *ticket) {
         t->ffW.assign(req->ff_water, req->ff_water + nq);
     }
     if (req->frame_weights) t->fw.assign(req->frame_weights, req->frame_weights + nf);
+    if (req->n_lattices) t->lats.assign(req->lattices, req->lattices + req->n_lattices);
     t->req = *req;
+    t->req.lattices = t->lats.empty() ? nullptr : t->lats.data();
     t->req.xyz = t->xyz.data();
     t->req.species = t->species.data();
     t->req.ff_atoms = t->ffA.data();

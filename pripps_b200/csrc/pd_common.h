@@ -80,3 +80,25 @@ struct PdPairDev {
     int32_t a, b;
     double q0[4];
 };
+
+// A lattice set of one class: its points are origin + spacing·(i, j, k); the
+// class's self pair sums come from the exact pair count per integer squared
+// offset n = |Δ(i, j, k)|², hist[hist_off + n], n < n_bins.
+struct PdLatDev {
+    double origin[3];
+    double spacing;
+    int32_t ext[3];
+    int32_t cls;       // class index
+    int32_t start;     // padded index of the class's first point
+    int32_t n;         // points of the class
+    int32_t pair;      // class-pair index (cls, cls)
+    int32_t n_bins;    // max n + 1
+    int64_t hist_off;  // first bin in the histogram array
+};
+
+// One CTA of the pair-count kernel: lattice `lat`, i points [i0, i0 + 128)
+// of the class (relative to its start), j points [j0, j1), pairs with j > i.
+struct PdLatTile {
+    int32_t lat, i0, j0, j1;
+};
+static_assert(sizeof(PdLatTile) == 16, "PdLatTile layout");

@@ -328,6 +328,16 @@ __device__ __forceinline__ void pairs_range_x2(const float4 *__restrict__ at, fl
     }
 }
 
+// Pairs a thread adds in FP32 before the warp's partial sums go into its
+// FP64 slot. A j range of a tile is walked in sub-chunks of this length with
+// fresh FP32 accumulators: FP32 running sums over thousands of terms lose
+// ε·|running sum| per addition (and over same-sign terms that loss has a
+// sign), which on sums of 10^9 pairs that cancel to 10^-5 of their scale
+// shows up in the result; short FP32 runs keep it far below the profile.
+#ifndef PD_JFLUSH
+#define PD_JFLUSH 512
+#endif
+
 // Resident CTAs per SM each FP32 shape is compiled for (register budget
 // 65536 / (128 · blocks) per thread).
 constexpr int fp32_min_blocks(int K, int MODE, int NP) {
@@ -380,79 +390,85 @@ __global__ void __launch_bounds__(PD_THREADS, fp32_min_blocks(K, MODE, NP))
         const bool general_step = rq.dq * (2.0 * radius) > 0.78;
 
         if constexpr (PACKED) {
-            float2 acc[K / 2];
-#pragma unroll
-            for (int t = 0; t < K / 2; ++t) acc[t] = make_float2(0.0f, 0.0f);
             const float2 *q2 = reinterpret_cast<const float2 *>(s_qres);
             // 16-point chunks of this block that lie on the grid. The
             // small-q residual blocks (the first of a grid) run whole: a
             // tail check there costs the register spills it saves in steps.
             const int nchunk = (min(K, rq.nq - kq0) + 15) >> 4;
-            if (resid) {
-                if (general_step)
-                    pairs_range_x2<K, NP, true, true>(at, pi, i, ivalid, jb.j0, jb.j1, qs_hi,
-                                                      qs_lo, dq_hi, dq_lo, q2, acc,
-                                                        K / 16);
-                else
-                    pairs_range_x2<K, NP, true, false>(at, pi, i, ivalid, jb.j0, jb.j1, qs_hi,
-                                                       qs_lo, dq_hi, dq_lo, q2, acc,
-                                                        K / 16);
-            } else {
-                if (general_step)
-                    pairs_range_x2<K, NP, false, true>(at, pi, i, ivalid, jb.j0, jb.j1, qs_hi,
-                                                       qs_lo, dq_hi, dq_lo, q2, acc,
-                                                        nchunk);
-                else
-                    pairs_range_x2<K, NP, false, false>(at, pi, i, ivalid, jb.j0, jb.j1, qs_hi,
-                                                        qs_lo, dq_hi, dq_lo, q2, acc,
-                                                        nchunk);
-            }
-            // Warp-reduce and write this warp's slot: K FP64 values.
             double *slot = rq.slots + (jb.slot + warp) * static_cast<int64_t>(K);
+            for (int js = jb.j0; js < jb.j1; js += PD_JFLUSH) {
+                const int je = min(jb.j1, js + PD_JFLUSH);
+                float2 acc[K / 2];
 #pragma unroll
-            for (int t = 0; t < K / 2; ++t) {
-                const float v0 = warp_sum(acc[t].x);
-                const float v1 = warp_sum(acc[t].y);
-                if (lane == ((2 * t) & 31)) slot[2 * t] = static_cast<double>(v0);
-                if (lane == ((2 * t + 1) & 31)) slot[2 * t + 1] = static_cast<double>(v1);
+                for (int t = 0; t < K / 2; ++t) acc[t] = make_float2(0.0f, 0.0f);
+                if (resid) {
+                    if (general_step)
+                        pairs_range_x2<K, NP, true, true>(at, pi, i, ivalid, js, je, qs_hi, qs_lo,
+                                                          dq_hi, dq_lo, q2, acc, K / 16);
+                    else
+                        pairs_range_x2<K, NP, true, false>(at, pi, i, ivalid, js, je, qs_hi,
+                                                           qs_lo, dq_hi, dq_lo, q2, acc, K / 16);
+                } else {
+                    if (general_step)
+                        pairs_range_x2<K, NP, false, true>(at, pi, i, ivalid, js, je, qs_hi,
+                                                           qs_lo, dq_hi, dq_lo, q2, acc, nchunk);
+                    else
+                        pairs_range_x2<K, NP, false, false>(at, pi, i, ivalid, js, je, qs_hi,
+                                                            qs_lo, dq_hi, dq_lo, q2, acc, nchunk);
+                }
+                // Warp-reduce and add into this warp's slot: K FP64 values,
+                // in sub-chunk order (one warp owns the slot: deterministic).
+                const bool first = js == jb.j0;
+#pragma unroll
+                for (int t = 0; t < K / 2; ++t) {
+                    const float v0 = warp_sum(acc[t].x);
+                    const float v1 = warp_sum(acc[t].y);
+                    if (lane == ((2 * t) & 31))
+                        slot[2 * t] = (first ? 0.0 : slot[2 * t]) + static_cast<double>(v0);
+                    if (lane == ((2 * t + 1) & 31))
+                        slot[2 * t + 1] = (first ? 0.0 : slot[2 * t + 1]) + static_cast<double>(v1);
+                }
             }
         } else {
-            float acc[NACC][K];
-#pragma unroll
-            for (int a = 0; a < NACC; ++a)
-#pragma unroll
-                for (int k = 0; k < K; ++k) acc[a][k] = 0.0f;
-
-            if (resid) {
-                if (general_step)
-                    pairs_range<K, MODE, NP, true, true>(at, pi, i, ivalid, jb.j0, jb.j1, qs_hi,
-                                                         qs_lo, dq_hi, dq_lo, s_qres, acc);
-                else
-                    pairs_range<K, MODE, NP, true, false>(at, pi, i, ivalid, jb.j0, jb.j1, qs_hi,
-                                                          qs_lo, dq_hi, dq_lo, s_qres, acc);
-            } else {
-                if (general_step)
-                    pairs_range<K, MODE, NP, false, true>(at, pi, i, ivalid, jb.j0, jb.j1, qs_hi,
-                                                          qs_lo, dq_hi, dq_lo, s_qres, acc);
-                else
-                    pairs_range<K, MODE, NP, false, false>(at, pi, i, ivalid, jb.j0, jb.j1, qs_hi,
-                                                           qs_lo, dq_hi, dq_lo, s_qres, acc);
-            }
-
-            // Warp-reduce and write this warp's slot: [4][K] FP64 values.
             double *slot = rq.slots + (jb.slot + warp) * static_cast<int64_t>(K) * 4;
             const float wi = ivalid ? pi.w : 0.0f;
+            for (int js = jb.j0; js < jb.j1; js += PD_JFLUSH) {
+                const int je = min(jb.j1, js + PD_JFLUSH);
+                float acc[NACC][K];
 #pragma unroll
-            for (int k = 0; k < K; ++k) {
-                const float t0 = warp_sum(acc[0][k]);
-                const float ti = warp_sum(wi * acc[0][k]);
-                const float tj = warp_sum(acc[NACC - 1][k]);
-                const float tij = warp_sum(wi * acc[NACC - 1][k]);
-                if (lane == (k & 31)) {
-                    slot[k] = t0;
-                    slot[K + k] = ti;
-                    slot[2 * K + k] = tj;
-                    slot[3 * K + k] = tij;
+                for (int a = 0; a < NACC; ++a)
+#pragma unroll
+                    for (int k = 0; k < K; ++k) acc[a][k] = 0.0f;
+                if (resid) {
+                    if (general_step)
+                        pairs_range<K, MODE, NP, true, true>(at, pi, i, ivalid, js, je, qs_hi,
+                                                             qs_lo, dq_hi, dq_lo, s_qres, acc);
+                    else
+                        pairs_range<K, MODE, NP, true, false>(at, pi, i, ivalid, js, je, qs_hi,
+                                                              qs_lo, dq_hi, dq_lo, s_qres, acc);
+                } else {
+                    if (general_step)
+                        pairs_range<K, MODE, NP, false, true>(at, pi, i, ivalid, js, je, qs_hi,
+                                                              qs_lo, dq_hi, dq_lo, s_qres, acc);
+                    else
+                        pairs_range<K, MODE, NP, false, false>(at, pi, i, ivalid, js, je, qs_hi,
+                                                               qs_lo, dq_hi, dq_lo, s_qres, acc);
+                }
+                // Warp-reduce and add into this warp's slot: [4][K] FP64 values.
+                const bool first = js == jb.j0;
+#pragma unroll
+                for (int k = 0; k < K; ++k) {
+                    const float t0 = warp_sum(acc[0][k]);
+                    const float ti = warp_sum(wi * acc[0][k]);
+                    const float tj = warp_sum(acc[NACC - 1][k]);
+                    const float tij = warp_sum(wi * acc[NACC - 1][k]);
+                    if (lane == (k & 31)) {
+                        slot[k] = (first ? 0.0 : slot[k]) + static_cast<double>(t0);
+                        slot[K + k] = (first ? 0.0 : slot[K + k]) + static_cast<double>(ti);
+                        slot[2 * K + k] = (first ? 0.0 : slot[2 * K + k]) + static_cast<double>(tj);
+                        slot[3 * K + k] =
+                            (first ? 0.0 : slot[3 * K + k]) + static_cast<double>(tij);
+                    }
                 }
             }
         }
@@ -714,6 +730,112 @@ __global__ void pd_combine_terms(const double *__restrict__ pairsum,
     o[5 * nq + q] = CB;
 }
 
+// ------------------------------------------------------------ lattice sets
+// Integer lattice coordinates of every point of every lattice set, from the
+// FP64 input positions (frame 0): i = rint((x - origin)/spacing) per axis. A
+// point farther than 1e-6·spacing from its lattice node, or outside the
+// extents, sets *err (the profiles of the request then become NaN).
+__global__ void pd_lattice_index(const double *__restrict__ xyz, const int32_t *__restrict__ perm,
+                                 const PdLatDev *__restrict__ lat, int4 *__restrict__ idx,
+                                 int *__restrict__ err) {
+    const PdLatDev d = lat[blockIdx.y];
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < d.n; r += gridDim.x * blockDim.x) {
+        const int p = d.start + r;
+        const int64_t src = perm[p];
+        int c[3] = {0, 0, 0};  // an invalid point counts at the origin node (in range)
+        bool ok = src >= 0;
+        for (int a = 0; a < 3 && ok; ++a) {
+            const double x = xyz[3 * src + a];
+            const double u = (x - d.origin[a]) / d.spacing;
+            const double ur = rint(u);
+            ok = fabs(x - (d.origin[a] + ur * d.spacing)) <= 1e-6 * d.spacing && ur >= 0.0 &&
+                 ur < static_cast<double>(d.ext[a]);
+            c[a] = ok ? static_cast<int>(ur) : 0;
+        }
+        if (!ok) atomicOr(err, 1);
+        idx[p] = make_int4(c[0], c[1], c[2], 0);
+    }
+}
+
+// Exact pair counts per integer squared offset n = |Δ(i, j, k)|² of a
+// lattice set: one CTA per tile (128 i points, a range of j points, j > i),
+// counted in a shared-memory histogram (32-bit: a tile holds at most
+// 128 × 8192 pairs) and added to the FP64-free 64-bit global histogram at the
+// end. Integer sums: the counts do not depend on the order the CTAs run in.
+// With more bins than fit in shared memory (`shared_bins` = 0) the CTA adds
+// straight to the global histogram.
+__global__ void __launch_bounds__(128) pd_lattice_hist(const PdLatTile *__restrict__ tiles,
+                                                       const PdLatDev *__restrict__ lat,
+                                                       const int4 *__restrict__ idx,
+                                                       unsigned long long *__restrict__ hist,
+                                                       int shared_bins) {
+    extern __shared__ unsigned int s_hist[];
+    const PdLatTile t = tiles[blockIdx.x];
+    const PdLatDev d = lat[t.lat];
+    const bool use_shared = shared_bins > 0;
+    if (use_shared)
+        for (int b = threadIdx.x; b < d.n_bins; b += blockDim.x) s_hist[b] = 0u;
+    __syncthreads();
+    const int i = t.i0 + threadIdx.x;
+    if (i < d.n) {
+        const int4 a = idx[d.start + i];
+        for (int j = max(t.j0, i + 1); j < t.j1; ++j) {
+            const int4 b = idx[d.start + j];
+            const int dx = a.x - b.x, dy = a.y - b.y, dz = a.z - b.z;
+            const int n = dx * dx + dy * dy + dz * dz;  // < n_bins: both points in the extents
+            if (use_shared)
+                atomicAdd(&s_hist[n], 1u);
+            else
+                atomicAdd(&hist[d.hist_off + n], 1ull);
+        }
+    }
+    __syncthreads();
+    if (use_shared)
+        for (int b = threadIdx.x; b < d.n_bins; b += blockDim.x) {
+            const unsigned int v = s_hist[b];
+            if (v) atomicAdd(&hist[d.hist_off + b], static_cast<unsigned long long>(v));
+        }
+}
+
+// Self pair sums of the lattice sets from their pair counts:
+// Σ_{i<j} sinc(q r_ij) = Σ_n count(n)·sinc(q·spacing·√n), FP64, one CTA per
+// (q, lattice); each thread adds the bins n ≡ thread (mod 256) in ascending
+// order and a fixed tree adds the threads, so the sum is deterministic. The
+// value overwrites the class pair's entry of `pairsum` (the pair tiles skip
+// those pairs). Only the rank that adds the exact terms writes a sum; the
+// others write 0. *err set: NaN.
+__global__ void __launch_bounds__(256) pd_lattice_sums(const unsigned long long *__restrict__ hist,
+                                                       const PdLatDev *__restrict__ lat,
+                                                       const double *__restrict__ qv, int32_t nq,
+                                                       int32_t add_exact,
+                                                       const int *__restrict__ err,
+                                                       double *__restrict__ pairsum) {
+    __shared__ double s_part[256];
+    const int q = blockIdx.x;
+    const PdLatDev d = lat[blockIdx.y];
+    const double qval = qv[q];
+    double acc = 0.0;
+    for (int n = 1 + threadIdx.x; n < d.n_bins; n += 256) {
+        const unsigned long long c = hist[d.hist_off + n];
+        if (c == 0ull) continue;
+        const double x = qval * d.spacing * sqrt(static_cast<double>(n));
+        // sinc as the reference defines it (src/debye.rs:17-24)
+        const double sc = fabs(x) < 1e-8 ? 1.0 : sin(x) / x;
+        acc += static_cast<double>(c) * sc;
+    }
+    s_part[threadIdx.x] = acc;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if (threadIdx.x < w) s_part[threadIdx.x] += s_part[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        double v = add_exact ? s_part[0] : 0.0;
+        if (*err) v = __longlong_as_double(0x7ff8000000000000ll);  // NaN
+        pairsum[static_cast<int64_t>(d.pair) * nq + q] = v;
+    }
+}
+
 // Frame-weighted mean of the six profiles, frames added in order.
 __global__ void pd_frame_mean(const double *__restrict__ terms, const double *__restrict__ fw,
                               int32_t n_frames, int32_t nq, double *__restrict__ out) {
@@ -890,6 +1012,51 @@ cudaError_t launch_combine(const double *pairsum, const PdClassDev *cls, const P
     const int grid = static_cast<int>((total + 127) / 128);
     pd_combine_terms<<<grid, 128, 0, st>>>(pairsum, cls, pairs, n_cls, n_pairs, nq, nv, n_frames,
                                            ffA, ffC, ffW, add_diag, terms);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_lattice(const double *xyz, const int32_t *perm, const PdLatDev *lat_dev,
+                           const PdLatDev *lat_host, int n_lat, const PdLatTile *tiles,
+                           int64_t n_tiles, int4 *idx, unsigned long long *hist, int64_t n_bins,
+                           int *err, cudaStream_t st) {
+    if (n_lat == 0) return cudaSuccess;
+    cudaError_t e = cudaMemsetAsync(hist, 0, static_cast<size_t>(n_bins) * 8, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(err, 0, sizeof(int), st);
+    if (e != cudaSuccess) return e;
+    int max_n = 1, max_bins = 1;
+    for (int l = 0; l < n_lat; ++l) {
+        max_n = max(max_n, lat_host[l].n);
+        max_bins = max(max_bins, lat_host[l].n_bins);
+    }
+    const dim3 g1(static_cast<unsigned>(min((max_n + 255) / 256, 4096)), n_lat);
+    pd_lattice_index<<<g1, 256, 0, st>>>(xyz, perm, lat_dev, idx, err);
+    if ((e = cudaGetLastError()) != cudaSuccess || n_tiles == 0) return e;
+    // shared-memory histogram when the bins fit (opt-in limit of the device)
+    int dev = 0, smem_optin = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    const size_t need = static_cast<size_t>(max_bins) * 4;
+    int shared_bins = need <= static_cast<size_t>(smem_optin) ? max_bins : 0;
+    size_t smem = shared_bins ? need : 0;
+    if (smem > 48 * 1024) {
+        e = cudaFuncSetAttribute(pd_lattice_hist, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(smem));
+        if (e != cudaSuccess) {
+            (void)cudaGetLastError();
+            shared_bins = 0;
+            smem = 0;
+        }
+    }
+    pd_lattice_hist<<<static_cast<unsigned>(n_tiles), 128, smem, st>>>(tiles, lat_dev, idx, hist,
+                                                                        shared_bins);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_lattice_sums(const unsigned long long *hist, const PdLatDev *lat, int n_lat,
+                                const double *qv, int32_t nq, int add_exact, const int *err,
+                                double *pairsum, cudaStream_t st) {
+    if (n_lat == 0) return cudaSuccess;
+    pd_lattice_sums<<<dim3(nq, n_lat), 256, 0, st>>>(hist, lat, qv, nq, add_exact, err, pairsum);
     return cudaGetLastError();
 }
 

@@ -31,6 +31,16 @@ cudaError_t launch_combine(const double *pairsum, const PdClassDev *cls, const P
                            int32_t n_cls, int32_t n_pairs, int32_t nq, int32_t nv,
                            int32_t n_frames, const double *ffA, const double *ffC,
                            const double *ffW, int add_diag, double *terms, cudaStream_t st);
+// Lattice sets: integer coordinates of their points and the exact pair count
+// per squared offset (after pack), then their self pair sums (after the slot
+// reduction, overwriting those class pairs' entries of pairsum).
+cudaError_t launch_lattice(const double *xyz, const int32_t *perm, const PdLatDev *lat_dev,
+                           const PdLatDev *lat_host, int n_lat, const PdLatTile *tiles,
+                           int64_t n_tiles, int4 *idx, unsigned long long *hist, int64_t n_bins,
+                           int *err, cudaStream_t st);
+cudaError_t launch_lattice_sums(const unsigned long long *hist, const PdLatDev *lat, int n_lat,
+                                const double *qv, int32_t nq, int add_exact, const int *err,
+                                double *pairsum, cudaStream_t st);
 cudaError_t launch_frame_mean(const double *terms, const double *fw, int32_t n_frames, int32_t nq,
                               double *out, cudaStream_t st);
 cudaError_t launch_ffma_probe(float *out, int iters, int grid, int block, bool packed,

@@ -29,7 +29,12 @@ uint64_t Plan::device_bytes() const {
     const uint64_t sums = static_cast<uint64_t>(n_frames) * nv * n_pairs * nq * sizeof(double);
     const uint64_t terms = static_cast<uint64_t>(n_frames + 1) * 6 * nq * sizeof(double);
     const uint64_t misc = static_cast<uint64_t>(n_frames) * 5 * sizeof(double) + 4096;
-    return atoms + xyz_in + tables + layout + jb + slots + lists + sums + terms + misc;
+    const uint64_t latt = lat.empty() ? 0
+                                      : lat.size() * sizeof(PdLatDev) +
+                                            lat_tiles.size() * sizeof(PdLatTile) +
+                                            static_cast<uint64_t>(n_pad) * 16 +
+                                            static_cast<uint64_t>(lat_bins) * 8;
+    return atoms + xyz_in + tables + layout + jb + slots + lists + sums + terms + misc + latt;
 }
 
 int validate_request(const pd_request *req, bool device_pointers, std::string &msg) {
@@ -65,8 +70,41 @@ int validate_request(const pd_request *req, bool device_pointers, std::string &m
         msg = "ff_water is required when hyd_weights is given";
         return PD_EINVAL;
     }
-    if (req->flags != 0 || req->reserved != 0) {
-        msg = "flags and reserved must be 0";
+    if (req->flags != 0) {
+        msg = "flags must be 0";
+        return PD_EINVAL;
+    }
+    if (req->n_lattices > PD_MAX_LATTICES || (req->n_lattices && !req->lattices)) {
+        msg = "n_lattices must be <= " + std::to_string(PD_MAX_LATTICES) +
+              " with a lattices array";
+        return PD_EINVAL;
+    }
+    for (uint32_t l = 0; l < req->n_lattices; ++l) {
+        const pd_lattice &L = req->lattices[l];
+        if (L.species >= req->n_species || L.reserved || L.reserved2 ||
+            !(std::isfinite(L.spacing) && L.spacing > 0.0) || !std::isfinite(L.origin[0]) ||
+            !std::isfinite(L.origin[1]) || !std::isfinite(L.origin[2]) || L.extent[0] < 1 ||
+            L.extent[1] < 1 || L.extent[2] < 1 || L.extent[0] > (1u << 16) ||
+            L.extent[1] > (1u << 16) || L.extent[2] > (1u << 16)) {
+            msg = "lattice " + std::to_string(l) +
+                  ": species < n_species, spacing > 0, finite origin, extents in [1, 65536] "
+                  "and zero reserved fields required";
+            return PD_EINVAL;
+        }
+        const double e0 = L.extent[0] - 1.0, e1 = L.extent[1] - 1.0, e2 = L.extent[2] - 1.0;
+        if (e0 * e0 + e1 * e1 + e2 * e2 >= static_cast<double>(PD_MAX_LATTICE_BINS)) {
+            msg = "lattice " + std::to_string(l) + " is too large: its squared diagonal exceeds " +
+                  std::to_string(PD_MAX_LATTICE_BINS) + " grid steps²";
+            return PD_EINVAL;
+        }
+        for (uint32_t m = 0; m < l; ++m)
+            if (req->lattices[m].species == L.species) {
+                msg = "two lattices name species " + std::to_string(L.species);
+                return PD_EINVAL;
+            }
+    }
+    if (req->n_lattices && req->n_frames > 1) {
+        msg = "lattice sets need a single frame";
         return PD_EINVAL;
     }
     if (!std::isfinite(req->qmin) || !std::isfinite(req->qmax) || req->qmin < 0.0 ||
@@ -240,6 +278,36 @@ int build_plan(const pd_request *req, const uint32_t *species, const double *w,
             ++ci;
         }
     }
+    // ---- lattice sets: one class each, class mode only
+    std::vector<int> lat_of_cls(c, -1);
+    P.lat.clear();
+    for (uint32_t l = 0; l < req->n_lattices; ++l) {
+        const pd_lattice &L = req->lattices[l];
+        int found = -1, count = 0;
+        for (int k = 0; k < c; ++k)
+            if (P.cls[k].species == static_cast<int32_t>(L.species)) {
+                found = k;
+                ++count;
+            }
+        if (count == 0) continue;  // no point of the species: nothing to sum
+        if (count > 1 || P.mode != PD_MODE_CLASS) {
+            msg = "the points of lattice species " + std::to_string(L.species) +
+                  " must share one hydration weight (and the request have at most " +
+                  std::to_string(PD_MAX_CLASSES) + " species × weight classes)";
+            return PD_EINVAL;
+        }
+        PdLatDev d{};
+        for (int a = 0; a < 3; ++a) {
+            d.origin[a] = L.origin[a];
+            d.ext[a] = static_cast<int32_t>(L.extent[a]);
+        }
+        d.spacing = L.spacing;
+        d.cls = found;
+        const int64_t e0 = L.extent[0] - 1, e1 = L.extent[1] - 1, e2 = L.extent[2] - 1;
+        d.n_bins = static_cast<int32_t>(e0 * e0 + e1 * e1 + e2 * e2 + 1);
+        lat_of_cls[found] = static_cast<int>(P.lat.size());
+        P.lat.push_back(d);
+    }
     std::vector<int32_t> atom_cls(n);
     std::vector<std::vector<int32_t>> members(c);
     for (int64_t i = 0; i < n; ++i) {
@@ -319,6 +387,25 @@ int build_plan(const pd_request *req, const uint32_t *species, const double *w,
             P.pairs.push_back(pd);
         }
     P.n_pairs = static_cast<int>(P.pairs.size());
+    // lattice layout: class range, self pair, histogram bins, count tiles
+    {
+        int64_t off = 0;
+        P.lat_tiles.clear();
+        for (size_t l = 0; l < P.lat.size(); ++l) {
+            PdLatDev &d = P.lat[l];
+            d.start = P.cls_start[d.cls];
+            d.n = static_cast<int32_t>(members[d.cls].size());
+            d.pair = pair_index[d.cls * c + d.cls];
+            d.hist_off = off;
+            off += d.n_bins;
+            for (int32_t i0 = 0; i0 < d.n; i0 += PD_LAT_IBLOCK)
+                for (int32_t j0 = i0; j0 < d.n; j0 += PD_LAT_JCHUNK)
+                    if (std::min(d.n, j0 + PD_LAT_JCHUNK) - 1 > i0)
+                        P.lat_tiles.push_back(PdLatTile{static_cast<int32_t>(l), i0, j0,
+                                                        std::min(d.n, j0 + PD_LAT_JCHUNK)});
+        }
+        P.lat_bins = off;
+    }
 
     // ---- tiles of one frame, in creation order
     const int K = P.tun.K, TJ = P.tun.TJ;
@@ -343,6 +430,16 @@ int build_plan(const pd_request *req, const uint32_t *species, const double *w,
             const int32_t cend = P.cls_start[k] + static_cast<int32_t>(members[k].size());
             const int32_t s0 = std::max(i0, P.cls_start[k]);
             if (cend - 1 <= i0) continue;  // no j > the block's first atom
+            if (lat_of_cls[k] >= 0) {
+                // a lattice class's self pairs come from its pair counts: drop
+                // the tiles whose i atoms all belong to it
+                bool all_k = true;
+                for (int wv = 0; wv < PD_WARPS; ++wv) {
+                    const int g = ib * PD_WARPS + wv;
+                    if (P.gvalid[g] > 0 && P.gclass[g] != k) all_k = false;
+                }
+                if (all_k) continue;
+            }
             for (int32_t j0 = s0; j0 < cend; j0 += TJ)
                 tiles.push_back(Tile{i0, j0, std::min(cend, j0 + TJ), k});
         }
@@ -374,6 +471,7 @@ int build_plan(const pd_request *req, const uint32_t *species, const double *w,
                 const int g = t.i0 / PD_GRANULE + wv;
                 const int a = P.gclass[g];
                 if (a < 0 || P.gvalid[g] == 0 || a > t.cls) continue;
+                if (a == t.cls && lat_of_cls[a] >= 0) continue;  // from the pair counts
                 const int64_t ilo = static_cast<int64_t>(g) * PD_GRANULE;
                 const int64_t ihi = ilo + P.gvalid[g];  // exclusive
                 if (t.j1 - 1 <= ilo) continue;          // every j <= every i
@@ -388,6 +486,8 @@ int build_plan(const pd_request *req, const uint32_t *species, const double *w,
             }
         }
     }
+    for (const PdLatDev &d : P.lat)
+        covered += static_cast<uint64_t>(d.n) * static_cast<uint64_t>(d.n - 1) / 2;
     P.pairs_covered = covered;
     P.lptr.assign(static_cast<size_t>(P.n_pairs) * P.nqb + 1, 0);
     for (size_t e = 0; e < lists.size(); ++e) P.lptr[e + 1] = P.lptr[e] + lists[e].size();

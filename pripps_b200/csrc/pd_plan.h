@@ -13,6 +13,13 @@ namespace pd {
 // At most this many (species, hydration weight) classes use the one-
 // accumulator class mode; more distinct weights switch to the weighted mode.
 constexpr int PD_MAX_CLASSES = 48;
+// Lattice sets per request, and the largest squared grid diagonal (bins of
+// its pair-count histogram).
+constexpr uint32_t PD_MAX_LATTICES = 8;
+constexpr int64_t PD_MAX_LATTICE_BINS = int64_t{1} << 24;
+// Pair-count tiles: 128 i points × up to 8192 j points.
+constexpr int PD_LAT_IBLOCK = 128;
+constexpr int PD_LAT_JCHUNK = 8192;
 
 struct Tuning {
     int K = 64;     // q-block length
@@ -52,6 +59,12 @@ struct Plan {
     std::vector<int64_t> lptr;  // [n_pairs * nqb + 1]
     std::vector<int64_t> lidx;  // slot indices within a frame
     uint64_t pairs_covered = 0; // per frame, unordered pairs over all tiles
+
+    // lattice sets (class mode, one frame): their self pairs are counted per
+    // integer squared offset instead of running through the pair tiles
+    std::vector<PdLatDev> lat;
+    std::vector<PdLatTile> lat_tiles;
+    int64_t lat_bins = 0;
 
     // device memory the plan needs, in bytes
     uint64_t device_bytes() const;

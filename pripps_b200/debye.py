@@ -110,6 +110,9 @@ class DebyeRequest:
     nq: int
     frame_weights: Optional[np.ndarray] = None
     precision: str = "fp32"
+    # lattice sets: (species, origin [3], spacing, extent [3]) per set whose
+    # points all sit on that lattice (see pd_lattice in pripps_debye.h)
+    lattices: Optional[list] = None
 
     def __post_init__(self):
         self.xyz = np.ascontiguousarray(self.xyz, dtype=np.float64)
@@ -148,7 +151,17 @@ class DebyeRequest:
         r.n_frames = self.n_frames if self.xyz.ndim == 3 else 0
         r.frame_weights = _lib.dptr(self.frame_weights)
         r.flags = 0
-        r.reserved = 0
+        lats = self.lattices or []
+        r.n_lattices = len(lats)
+        if lats:
+            arr = (_lib.PdLattice * len(lats))()
+            for k, (sp, origin, spacing, extent) in enumerate(lats):
+                arr[k].species = int(sp)
+                arr[k].origin[:] = [float(v) for v in origin]
+                arr[k].spacing = float(spacing)
+                arr[k].extent[:] = [int(v) for v in extent]
+            self._lattice_array = arr  # keep alive as long as the struct is used
+            r.lattices = C.cast(arr, C.POINTER(_lib.PdLattice))
         return r
 
 
@@ -220,6 +233,9 @@ def union_request(pos: np.ndarray, species: np.ndarray, ffA: np.ndarray,
         nxt += rows.shape[0]
         has_c = True
     has_b = hw is not None
+    lattices = []
+    if exc is not None and len(exc) and exc.lattice is not None and len(rows_c[-1]) == 1:
+        lattices.append((nxt - 1,) + tuple(exc.lattice))
     if hyd is not None and len(hyd):
         xyz.append(hyd.positions)
         sp.append(np.full(len(hyd), nxt, dtype=np.int64))
@@ -227,12 +243,14 @@ def union_request(pos: np.ndarray, species: np.ndarray, ffA: np.ndarray,
         rows_c.append(np.zeros((1, nq)))
         wts.append(hyd.weights)
         water = np.array([hyd.form_factors[0].eval(float(q)) for q in q_values])
+        if hyd.lattice is not None and np.all(hyd.weights == hyd.weights[0]):
+            lattices.append((nxt,) + tuple(hyd.lattice))
         nxt += 1
         has_b = True
     return DebyeRequest(np.concatenate(xyz), np.concatenate(sp).astype(np.uint32),
                         np.vstack(rows_a), np.vstack(rows_c) if has_c else None,
                         np.concatenate(wts) if has_b else None, water if has_b else None,
-                        qmin, qmax, len(q_values), None, precision)
+                        qmin, qmax, len(q_values), None, precision, lattices or None)
 
 
 def solve(req: DebyeRequest, ctx: Optional[_lib.Context] = None) -> np.ndarray:

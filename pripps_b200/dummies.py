@@ -44,8 +44,13 @@ class DummySet:
     a weight per dummy)."""
 
     def __init__(self, positions, *, form_factors: Sequence[FormFactor],
-                 kinds: Optional[np.ndarray] = None, weights: Optional[np.ndarray] = None):
+                 kinds: Optional[np.ndarray] = None, weights: Optional[np.ndarray] = None,
+                 lattice: Optional[tuple] = None):
         self.positions = np.ascontiguousarray(positions, dtype=np.float64).reshape(-1, 3)
+        # (origin [3], spacing, extent [3]) when every dummy sits on the grid
+        # origin + spacing·(i, j, k), 0 <= i < extent[0], ...: the device then
+        # sums the set's self pairs from exact counts per squared offset
+        self.lattice = lattice
         self.form_factors = list(form_factors)
         n = len(self.positions)
         if (kinds is None) == (weights is None):
@@ -69,8 +74,9 @@ class DummySet:
                 raise InternalError("DummySet: form factor index out of range")
 
     @classmethod
-    def weighted(cls, positions, form_factor: FormFactor, weights) -> "DummySet":
-        return cls(positions, form_factors=[form_factor], weights=weights)
+    def weighted(cls, positions, form_factor: FormFactor, weights,
+                 lattice: Optional[tuple] = None) -> "DummySet":
+        return cls(positions, form_factors=[form_factor], weights=weights, lattice=lattice)
 
     @classmethod
     def per_dummy(cls, positions, form_factors: Sequence[FormFactor], kinds) -> "DummySet":
@@ -122,13 +128,14 @@ def grid_steps(lo: float, hi: float, spacing: float) -> int:
     return int(math.ceil((hi - lo) / spacing)) + 1
 
 
-def _grid(lo: np.ndarray, hi: np.ndarray, spacing: float) -> np.ndarray:
+def _grid(lo: np.ndarray, hi: np.ndarray, spacing: float):
     """Grid points lo + i·spacing in the reference's loop order (x outer,
-    z inner), [nx·ny·nz, 3]."""
-    axes = [lo[d] + np.arange(grid_steps(lo[d], hi[d], spacing), dtype=np.float64) * spacing
-            for d in range(3)]
+    z inner), [nx·ny·nz, 3], and the lattice (lo, spacing, (nx, ny, nz))."""
+    ext = tuple(grid_steps(lo[d], hi[d], spacing) for d in range(3))
+    axes = [lo[d] + np.arange(ext[d], dtype=np.float64) * spacing for d in range(3)]
     gx, gy, gz = np.meshgrid(*axes, indexing="ij")
-    return np.stack([gx.ravel(), gy.ravel(), gz.ravel()], axis=1)
+    pts = np.stack([gx.ravel(), gy.ravel(), gz.ravel()], axis=1)
+    return pts, (tuple(float(v) for v in lo), float(spacing), ext)
 
 
 def nearest_surface_distance(points: np.ndarray, centers: np.ndarray, radii: np.ndarray,
@@ -173,10 +180,10 @@ def grid_excluded_dummies(pos: np.ndarray, ids: np.ndarray, formfactors: FormFac
         return DummySet.weighted(np.zeros((0, 3)), ff, np.zeros(0))
     margin = float(radii.max()) + spacing
     lo, hi = pos.min(axis=0) - margin, pos.max(axis=0) + margin
-    pts = _grid(lo, hi, spacing)
+    pts, lattice = _grid(lo, hi, spacing)
     d = nearest_surface_distance(pts, pos, radii, 0.0)
     keep = pts[d <= 0.0]
-    return DummySet.weighted(keep, ff, np.ones(len(keep)))
+    return DummySet.weighted(keep, ff, np.ones(len(keep)), lattice)
 
 
 def grid_hydration_dummies(pos: np.ndarray, ids: np.ndarray, formfactors: FormFactorMap,
@@ -194,8 +201,8 @@ def grid_hydration_dummies(pos: np.ndarray, ids: np.ndarray, formfactors: FormFa
         return DummySet.weighted(np.zeros((0, 3)), water, np.zeros(0))
     margin = float(radii.max()) + probe + thickness + spacing
     lo, hi = pos.min(axis=0) - margin, pos.max(axis=0) + margin
-    pts = _grid(lo, hi, spacing)
+    pts, lattice = _grid(lo, hi, spacing)
     outer = probe + thickness
     d = nearest_surface_distance(pts, pos, radii, outer)
     keep = pts[(d > probe) & (d < outer)]
-    return DummySet.weighted(keep, water, np.full(len(keep), per_cell))
+    return DummySet.weighted(keep, water, np.full(len(keep), per_cell), lattice)

@@ -182,3 +182,62 @@ def test_union_request_layout():
     assert np.all(req.ff_atoms[S:] == 0) and np.all(req.ff_excluded[:S] == 0)
     assert np.all(req.hyd_weights[:n] == 0)
     assert np.all(req.species[:n] < S)
+
+
+def _inspect(req):
+    import ctypes as C
+    from pripps_b200 import _lib
+    r = req.c_struct()
+    out = [C.c_uint64() for _ in range(4)]
+    rc = _lib.lib().pd_plan_inspect(None, C.byref(r), *[C.byref(o) for o in out])
+    return rc, [o.value for o in out]
+
+
+def test_union_request_marks_grid_sets_as_lattices_and_covers_every_pair():
+    """Both grid sets travel as lattice sets (one species each, the grid's
+    origin, spacing and extents); the plan's pair tiles plus the lattice
+    pair counts cover every unordered pair of the union exactly once, with
+    far fewer tiles than without the lattices."""
+    m, s, q = _grid_case(200, 6)
+    cfg = SolventConfig(ExcludedVolume.grid(1.0), Hydration.grid(0.03))
+    req = make_request(s, m, q, 0.0, 0.6, cfg, "fp32")
+    S = len(np.unique(s.ids))
+    assert [l[0] for l in req.lattices] == [S, S + 1]
+    for sp, origin, spacing, extent in req.lattices:
+        pts = req.xyz[req.species == sp]
+        idx = (pts - np.array(origin)) / spacing
+        assert np.all(np.abs(idx - np.rint(idx)) < 1e-9)
+        assert np.all(np.rint(idx) >= 0) and np.all(np.rint(idx) < np.array(extent))
+    rc, (ncls, npad, ntiles, covered) = _inspect(req)
+    assert rc == 0
+    n = req.n_atoms
+    assert covered == n * (n - 1) // 2
+    plain = make_request(s, m, q, 0.0, 0.6, cfg, "fp32")
+    plain.lattices = None
+    rc, (_, _, ntiles_plain, covered_plain) = _inspect(plain)
+    assert rc == 0 and covered_plain == covered
+    assert ntiles < ntiles_plain / 2
+
+
+def test_lattice_validation():
+    from pripps_b200 import _lib
+    m, s, q = _grid_case(60, 1)
+    cfg = SolventConfig(ExcludedVolume.grid(1.2), Hydration.grid(0.03))
+    good = make_request(s, m, q, 0.0, 0.6, cfg, "fp32")
+    assert _inspect(good)[0] == 0
+    sp, origin, spacing, extent = good.lattices[0]
+    for bad in [(sp, origin, -1.0, extent), (sp, origin, spacing, (0, 1, 1)),
+                (999, origin, spacing, extent), (sp, (np.nan, 0, 0), spacing, extent),
+                (sp, origin, spacing, (5000, 5000, 5000))]:
+        r = make_request(s, m, q, 0.0, 0.6, cfg, "fp32")
+        r.lattices = [bad]
+        assert _inspect(r)[0] == _lib.PD_EINVAL, bad
+    r = make_request(s, m, q, 0.0, 0.6, cfg, "fp32")
+    r.lattices = [good.lattices[0], good.lattices[0]]
+    assert _inspect(r)[0] == _lib.PD_EINVAL
+    # a lattice species whose points carry two hydration weights
+    r = make_request(s, m, q, 0.0, 0.6, cfg, "fp32")
+    hyd_sp = good.lattices[1][0]
+    k = np.flatnonzero(r.species == hyd_sp)[0]
+    r.hyd_weights[k] *= 2.0
+    assert _inspect(r)[0] == _lib.PD_EINVAL

@@ -1,7 +1,9 @@
 """Solvent dummies at their own positions on the device: the union request
 (atoms + grid excluded-volume cells + grid hydration points) through the C
 ABI against the oracle's build_model with the three sets kept apart
-(src/debye.rs:83-130), in both precision forms.
+(src/debye.rs:83-130), in both precision forms. The grid sets travel as
+lattice sets: their self sums come from exact pair counts per squared
+lattice offset, everything else from the pair kernels.
 
 Tolerances as for the colocated path: FP64 form 1e-10, FP32 form 1e-5 per
 profile (cross profiles normalised by sqrt(self_a·self_b))."""
@@ -18,7 +20,7 @@ pytestmark = pytest.mark.gpu
 TOL = {"fp64": 1e-10, "fp32": 1e-5}
 
 
-@pytest.mark.parametrize("precision", ["fp64"])
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
 @pytest.mark.parametrize("n,seed,spacing,nq,qmax", [(300, 3, 1.3, 60, 0.6), (120, 8, 1.0, 37, 0.9),
                                                     (700, 5, 1.6, 130, 0.5)])
 def test_grid_solvent_against_separate_sets(gpu_ctx, precision, n, seed, spacing, nq, qmax):
@@ -31,8 +33,6 @@ def test_grid_solvent_against_separate_sets(gpu_ctx, precision, n, seed, spacing
     assert np.all(err < TOL[precision]), err
 
 
-@pytest.mark.skip(reason="FP32 form on lattice dummy sets: exactly repeated distances make the "
-                         "recurrence's rounding coherent")
 def test_grid_solvent_10k_fp32_vs_fp64(gpu_ctx):
     """The 10,000-atom sphere with 1 Å grid excluded volume and a grid
     hydration shell (~111,000 points, nq = 500): FP32 form within 1e-5 of the
@@ -79,3 +79,30 @@ def test_trajectory_with_grid_solvent_rebuilds_dummies_per_frame(gpu_ctx):
         ref += wf * combine(solve(req, gpu_ctx), 1.05, 0.02)
     ref /= wts.sum()
     assert np.max(np.abs(got.total - ref) / np.abs(ref)) < 1e-12
+
+
+def test_point_off_its_lattice_is_refused(gpu_ctx):
+    """A lattice species with a point moved off the grid: the device flags it
+    and the solve returns PD_EINVAL instead of a result."""
+    from pripps_b200.errors import ValidationError
+    g = workloads.small_globule(150, 2).globule
+    req = workloads.grid_solvent_request(g, 0.0, 0.5, 20, "fp32", 1.2)
+    sp = req.lattices[1][0]
+    k = np.flatnonzero(req.species == sp)[3]
+    req.xyz[k, 0] += 0.01
+    with pytest.raises(ValidationError):
+        solve(req, gpu_ctx)
+    # and a correct request on the same context still solves
+    ok = workloads.grid_solvent_request(g, 0.0, 0.5, 20, "fp32", 1.2)
+    assert np.all(np.isfinite(solve(ok, gpu_ctx)))
+
+
+def test_lattice_sums_equal_pair_kernel_sums_in_fp64(gpu_ctx):
+    """The lattice path against the plain FP64 pair kernel on the same union
+    (lattices removed from the request): every profile within 1e-12."""
+    g = workloads.small_globule(500, 4).globule
+    req = workloads.grid_solvent_request(g, 0.0, 0.7, 90, "fp64", 1.1)
+    a = solve(req, gpu_ctx)
+    req.lattices = None
+    b = solve(req, gpu_ctx)
+    assert np.all(term_errors(a, b) < 1e-12), term_errors(a, b)
