@@ -955,7 +955,8 @@ int pd_ctx_create(int device, uint64_t mem_budget_bytes, pd_ctx **out) {
     size_t free_b = 0, total_b = 0;
     cudaMemGetInfo(&free_b, &total_b);
     ctx->budget = mem_budget_bytes ? mem_budget_bytes : static_cast<uint64_t>(free_b * 0.9);
-    e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+    e = pd::prepare_pair_kernels();
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) {
         cudaMemPoolProps pp{};
         pp.allocType = cudaMemAllocationTypePinned;
@@ -1639,6 +1640,12 @@ NoallocDevice *noalloc_device(int dev, int *rc) {
     nd.ctx = std::make_unique<pd_ctx>();
     nd.ctx->device = dev;
     nd.ctx->sm_count = sms;
+    e = pd::prepare_pair_kernels();  // launch attributes, before any capture
+    if (e != cudaSuccess) {
+        *rc = noalloc_fail(PD_EDEVICE, std::string("pd_solve_noalloc: kernel set-up failed: ") +
+                                           cudaGetErrorString(e));
+        return nullptr;
+    }
     return &g_noalloc.emplace(dev, std::move(nd)).first->second;
 }
 

@@ -20,6 +20,7 @@
 // every pair and q, and FP64 accumulation throughout.
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <cstdio>
 
@@ -183,6 +184,50 @@ __host__ __device__ __forceinline__ bool residual_q(double q, double radius) {
     return q * (2.0 * radius) < 2.0;
 }
 
+// ------------------------------------------------- shared-memory staging (TMA)
+// One-dimensional bulk copies (cp.async.bulk, no multicast) of j-atom chunks
+// into shared memory, completed on an mbarrier. Every wait is bounded: a
+// copy that does not land within ~2^22 polls makes the wait return false and
+// the caller poisons its results with NaN instead of hanging the GPU.
+__device__ __forceinline__ uint32_t smem_addr(const void *p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count)
+                 : "memory");
+}
+__device__ __forceinline__ void mbar_init_fence() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+// Thread 0 only: `bytes` (a multiple of 16, <= 2^20) from global `src`
+// (16-byte aligned) to shared `dst` (16-byte aligned), completing on `bar`.
+__device__ __forceinline__ void bulk_copy_to_shared(void *dst, const void *src, uint32_t bytes,
+                                                    unsigned long long *bar) {
+    // order earlier generic-proxy reads of dst before the async-proxy write
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
+                 "r"(bytes)
+                 : "memory");
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+            "r"(smem_addr(dst)),
+        "l"(src), "r"(bytes), "r"(smem_addr(bar))
+        : "memory");
+}
+__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, uint32_t phase) {
+    for (int it = 0; it < (1 << 22); ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+            " selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(done)
+            : "r"(smem_addr(bar)), "r"(phase)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
 // ---------------------------------------------------------------- K1 (FP32)
 // Seeds of NP consecutive j atoms (clamped reads past the range are masked).
 template <int MODE, int NP, bool RESID, bool GENERAL_STEP>
@@ -191,16 +236,17 @@ struct SeedGroup {
     float wj[NP];
     float vsum, vwsum;
 
-    __device__ __forceinline__ void make(const float4 *__restrict__ at, float4 pi, int i,
-                                         bool ivalid, int j, int j1, float qs_hi, float qs_lo,
-                                         float dq_hi, float dq_lo) {
+    // `at` holds the atoms [jbase, j1) (a chunk staged in shared memory).
+    __device__ __forceinline__ void make(const float4 *__restrict__ at, int jbase, float4 pi,
+                                         int i, bool ivalid, int j, int j1, float qs_hi,
+                                         float qs_lo, float dq_hi, float dq_lo) {
         vsum = 0.0f;
         vwsum = 0.0f;
 #pragma unroll
         for (int p = 0; p < NP; ++p) {
             const int jj = j + p;
             const bool inr = jj < j1;
-            const float4 pj = __ldg(at + (inr ? jj : j1 - 1));
+            const float4 pj = at[(inr ? jj : j1 - 1) - jbase];
             const bool valid = ivalid && inr && (jj > i);
             S[p] = pair_seed<GENERAL_STEP>(pi, pj, valid, qs_hi, qs_lo, dq_hi, dq_lo);
             if (MODE == PD_MODE_WEIGHTED) wj[p] = pj.w;
@@ -218,8 +264,8 @@ struct SeedGroup {
 // chains (sqrt, reductions, polynomials) overlap the recurrence instead of
 // stalling the warp between passes.
 template <int K, int MODE, int NP, bool RESID, bool GENERAL_STEP>
-__device__ __forceinline__ void pairs_range(const float4 *__restrict__ at, float4 pi, int i,
-                                            bool ivalid, int j0, int j1, float qs_hi,
+__device__ __forceinline__ void pairs_range(const float4 *__restrict__ at, int jbase, float4 pi,
+                                            int i, bool ivalid, int j0, int j1, float qs_hi,
                                             float qs_lo, float dq_hi, float dq_lo,
                                             const float *__restrict__ s_qres,
                                             float (&acc)[(MODE == PD_MODE_WEIGHTED) ? 2 : 1][K]) {
@@ -227,10 +273,10 @@ __device__ __forceinline__ void pairs_range(const float4 *__restrict__ at, float
     static_assert(K % 4 == 0, "K must be a multiple of 4");
     if (j0 >= j1) return;
     SeedGroup<MODE, NP, RESID, GENERAL_STEP> cur;
-    cur.make(at, pi, i, ivalid, j0, j1, qs_hi, qs_lo, dq_hi, dq_lo);
+    cur.make(at, jbase, pi, i, ivalid, j0, j1, qs_hi, qs_lo, dq_hi, dq_lo);
     for (int j = j0; j < j1; j += NP) {
         SeedGroup<MODE, NP, RESID, GENERAL_STEP> nxt;  // unused after the last pass
-        nxt.make(at, pi, i, ivalid, j + NP, j1, qs_hi, qs_lo, dq_hi, dq_lo);
+        nxt.make(at, jbase, pi, i, ivalid, j + NP, j1, qs_hi, qs_lo, dq_hi, dq_lo);
         float we_w[NP], wo_w[NP];
         if (MODE == PD_MODE_WEIGHTED) {
 #pragma unroll
@@ -289,18 +335,18 @@ __device__ __forceinline__ void pairs_range(const float4 *__restrict__ at, float
 // per chunk in a single code path measured faster on B200 than a separate
 // copy of the loop for tail blocks, which raised register spills.)
 template <int K, int NP, bool RESID, bool GENERAL_STEP>
-__device__ __forceinline__ void pairs_range_x2(const float4 *__restrict__ at, float4 pi, int i,
-                                               bool ivalid, int j0, int j1, float qs_hi,
+__device__ __forceinline__ void pairs_range_x2(const float4 *__restrict__ at, int jbase, float4 pi,
+                                               int i, bool ivalid, int j0, int j1, float qs_hi,
                                                float qs_lo, float dq_hi, float dq_lo,
                                                const float2 *__restrict__ s_qres2,
                                                float2 (&acc)[K / 2], int nchunk) {
     static_assert(K % 16 == 0, "K must be a multiple of 16");
     if (j0 >= j1) return;
     SeedGroup<PD_MODE_CLASS, NP, RESID, GENERAL_STEP> cur;
-    cur.make(at, pi, i, ivalid, j0, j1, qs_hi, qs_lo, dq_hi, dq_lo);
+    cur.make(at, jbase, pi, i, ivalid, j0, j1, qs_hi, qs_lo, dq_hi, dq_lo);
     for (int j = j0; j < j1; j += NP) {
         SeedGroup<PD_MODE_CLASS, NP, RESID, GENERAL_STEP> nxt;  // unused after the last pass
-        nxt.make(at, pi, i, ivalid, j + NP, j1, qs_hi, qs_lo, dq_hi, dq_lo);
+        nxt.make(at, jbase, pi, i, ivalid, j + NP, j1, qs_hi, qs_lo, dq_hi, dq_lo);
         float2 V[NP], D[NP], NA[NP], WE[NP], WO[NP];
 #pragma unroll
         for (int p = 0; p < NP; ++p) {
@@ -337,6 +383,15 @@ __device__ __forceinline__ void pairs_range_x2(const float4 *__restrict__ at, fl
 #ifndef PD_JFLUSH
 #define PD_JFLUSH 512
 #endif
+// j atoms per bulk copy into shared memory (two buffers of PD_JSTAGE float4,
+// 64 KB of dynamic shared memory per CTA); a multiple of PD_JFLUSH. One CTA
+// barrier per stage releases the buffer for the next copy.
+#ifndef PD_JSTAGE_ATOMS
+#define PD_JSTAGE_ATOMS 2048
+#endif
+constexpr int PD_JSTAGE = PD_JSTAGE_ATOMS;
+static_assert(PD_JSTAGE % PD_JFLUSH == 0, "stage must hold whole sub-chunks");
+constexpr size_t PD_FP32_DYN_SMEM = 2 * PD_JSTAGE * sizeof(float4);
 
 // Resident CTAs per SM each FP32 shape is compiled for (register budget
 // 65536 / (128 · blocks) per thread).
@@ -355,9 +410,21 @@ __global__ void __launch_bounds__(PD_THREADS, fp32_min_blocks(K, MODE, NP))
     constexpr bool PACKED = (MODE == PD_MODE_CLASS);
     __shared__ int s_job;
     __shared__ __align__(16) float s_qres[K];
+    // j atoms of the current and the next stage, staged by bulk copies
+    // (PD_FP32_DYN_SMEM bytes of dynamic shared memory)
+    extern __shared__ __align__(128) float4 pd_dyn_atoms[];
+    float4 *s_atoms[2] = {pd_dyn_atoms, pd_dyn_atoms + PD_JSTAGE};
+    __shared__ __align__(8) unsigned long long s_bar[2];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const int n_jobs = *n_jobs_ptr;
+    if (threadIdx.x == 0) {
+        mbar_init(&s_bar[0], 1);
+        mbar_init(&s_bar[1], 1);
+        mbar_init_fence();
+    }
+    __syncthreads();
+    uint32_t phase = 0;  // bit b: parity of buffer b's next completion
     for (;;) {
         if (threadIdx.x == 0) s_job = atomicAdd(counter, 1);
         __syncthreads();
@@ -396,44 +463,83 @@ __global__ void __launch_bounds__(PD_THREADS, fp32_min_blocks(K, MODE, NP))
             // tail check there costs the register spills it saves in steps.
             const int nchunk = (min(K, rq.nq - kq0) + 15) >> 4;
             double *slot = rq.slots + (jb.slot + warp) * static_cast<int64_t>(K);
-            for (int js = jb.j0; js < jb.j1; js += PD_JFLUSH) {
-                const int je = min(jb.j1, js + PD_JFLUSH);
+            const int nstage = (jb.j1 - jb.j0 + PD_JSTAGE - 1) / PD_JSTAGE;
+            if (threadIdx.x == 0 && nstage > 0)
+                bulk_copy_to_shared(s_atoms[0], at + jb.j0,
+                                    static_cast<uint32_t>(min(jb.j1 - jb.j0, PD_JSTAGE)) * 16,
+                                    &s_bar[0]);
+            for (int stg = 0; stg < nstage; ++stg) {
+              const int jss = jb.j0 + stg * PD_JSTAGE;
+              const int jse = min(jb.j1, jss + PD_JSTAGE);
+              if (threadIdx.x == 0 && stg + 1 < nstage)  // its buffer was released at stg - 1
+                  bulk_copy_to_shared(s_atoms[(stg + 1) & 1], at + jse,
+                                      static_cast<uint32_t>(min(jb.j1 - jse, PD_JSTAGE)) * 16,
+                                      &s_bar[(stg + 1) & 1]);
+              const int b = stg & 1;
+              const bool landed = mbar_wait(&s_bar[b], (phase >> b) & 1u);
+              phase ^= 1u << b;
+              const float4 *chunk = s_atoms[b];
+              for (int js = jss; js < jse; js += PD_JFLUSH) {
+                const int je = min(jse, js + PD_JFLUSH);
                 float2 acc[K / 2];
 #pragma unroll
                 for (int t = 0; t < K / 2; ++t) acc[t] = make_float2(0.0f, 0.0f);
                 if (resid) {
                     if (general_step)
-                        pairs_range_x2<K, NP, true, true>(at, pi, i, ivalid, js, je, qs_hi, qs_lo,
-                                                          dq_hi, dq_lo, q2, acc, K / 16);
+                        pairs_range_x2<K, NP, true, true>(chunk, jss, pi, i, ivalid, js, je, qs_hi,
+                                                          qs_lo, dq_hi, dq_lo, q2, acc, K / 16);
                     else
-                        pairs_range_x2<K, NP, true, false>(at, pi, i, ivalid, js, je, qs_hi,
+                        pairs_range_x2<K, NP, true, false>(chunk, jss, pi, i, ivalid, js, je, qs_hi,
                                                            qs_lo, dq_hi, dq_lo, q2, acc, K / 16);
                 } else {
                     if (general_step)
-                        pairs_range_x2<K, NP, false, true>(at, pi, i, ivalid, js, je, qs_hi,
+                        pairs_range_x2<K, NP, false, true>(chunk, jss, pi, i, ivalid, js, je, qs_hi,
                                                            qs_lo, dq_hi, dq_lo, q2, acc, nchunk);
                     else
-                        pairs_range_x2<K, NP, false, false>(at, pi, i, ivalid, js, je, qs_hi,
+                        pairs_range_x2<K, NP, false, false>(chunk, jss, pi, i, ivalid, js, je, qs_hi,
                                                             qs_lo, dq_hi, dq_lo, q2, acc, nchunk);
                 }
                 // Warp-reduce and add into this warp's slot: K FP64 values,
                 // in sub-chunk order (one warp owns the slot: deterministic).
+                // A chunk that never landed poisons the slot with NaN.
                 const bool first = js == jb.j0;
+                const double bad = __any_sync(0xffffffffu, !landed)
+                                       ? __longlong_as_double(0x7ff8000000000000ll)
+                                       : 0.0;
 #pragma unroll
                 for (int t = 0; t < K / 2; ++t) {
                     const float v0 = warp_sum(acc[t].x);
                     const float v1 = warp_sum(acc[t].y);
                     if (lane == ((2 * t) & 31))
-                        slot[2 * t] = (first ? 0.0 : slot[2 * t]) + static_cast<double>(v0);
+                        slot[2 * t] = (first ? 0.0 : slot[2 * t]) + static_cast<double>(v0) + bad;
                     if (lane == ((2 * t + 1) & 31))
-                        slot[2 * t + 1] = (first ? 0.0 : slot[2 * t + 1]) + static_cast<double>(v1);
+                        slot[2 * t + 1] =
+                            (first ? 0.0 : slot[2 * t + 1]) + static_cast<double>(v1) + bad;
                 }
+              }
+              __syncthreads();  // every read of buffer b done before it is refilled
             }
         } else {
             double *slot = rq.slots + (jb.slot + warp) * static_cast<int64_t>(K) * 4;
             const float wi = ivalid ? pi.w : 0.0f;
-            for (int js = jb.j0; js < jb.j1; js += PD_JFLUSH) {
-                const int je = min(jb.j1, js + PD_JFLUSH);
+            const int nstage = (jb.j1 - jb.j0 + PD_JSTAGE - 1) / PD_JSTAGE;
+            if (threadIdx.x == 0 && nstage > 0)
+                bulk_copy_to_shared(s_atoms[0], at + jb.j0,
+                                    static_cast<uint32_t>(min(jb.j1 - jb.j0, PD_JSTAGE)) * 16,
+                                    &s_bar[0]);
+            for (int stg = 0; stg < nstage; ++stg) {
+              const int jss = jb.j0 + stg * PD_JSTAGE;
+              const int jse = min(jb.j1, jss + PD_JSTAGE);
+              if (threadIdx.x == 0 && stg + 1 < nstage)  // its buffer was released at stg - 1
+                  bulk_copy_to_shared(s_atoms[(stg + 1) & 1], at + jse,
+                                      static_cast<uint32_t>(min(jb.j1 - jse, PD_JSTAGE)) * 16,
+                                      &s_bar[(stg + 1) & 1]);
+              const int b = stg & 1;
+              const bool landed = mbar_wait(&s_bar[b], (phase >> b) & 1u);
+              phase ^= 1u << b;
+              const float4 *chunk = s_atoms[b];
+              for (int js = jss; js < jse; js += PD_JFLUSH) {
+                const int je = min(jse, js + PD_JFLUSH);
                 float acc[NACC][K];
 #pragma unroll
                 for (int a = 0; a < NACC; ++a)
@@ -441,21 +547,24 @@ __global__ void __launch_bounds__(PD_THREADS, fp32_min_blocks(K, MODE, NP))
                     for (int k = 0; k < K; ++k) acc[a][k] = 0.0f;
                 if (resid) {
                     if (general_step)
-                        pairs_range<K, MODE, NP, true, true>(at, pi, i, ivalid, js, je, qs_hi,
+                        pairs_range<K, MODE, NP, true, true>(chunk, jss, pi, i, ivalid, js, je, qs_hi,
                                                              qs_lo, dq_hi, dq_lo, s_qres, acc);
                     else
-                        pairs_range<K, MODE, NP, true, false>(at, pi, i, ivalid, js, je, qs_hi,
+                        pairs_range<K, MODE, NP, true, false>(chunk, jss, pi, i, ivalid, js, je, qs_hi,
                                                               qs_lo, dq_hi, dq_lo, s_qres, acc);
                 } else {
                     if (general_step)
-                        pairs_range<K, MODE, NP, false, true>(at, pi, i, ivalid, js, je, qs_hi,
+                        pairs_range<K, MODE, NP, false, true>(chunk, jss, pi, i, ivalid, js, je, qs_hi,
                                                               qs_lo, dq_hi, dq_lo, s_qres, acc);
                     else
-                        pairs_range<K, MODE, NP, false, false>(at, pi, i, ivalid, js, je, qs_hi,
+                        pairs_range<K, MODE, NP, false, false>(chunk, jss, pi, i, ivalid, js, je, qs_hi,
                                                                qs_lo, dq_hi, dq_lo, s_qres, acc);
                 }
                 // Warp-reduce and add into this warp's slot: [4][K] FP64 values.
                 const bool first = js == jb.j0;
+                const double bad = __any_sync(0xffffffffu, !landed)
+                                       ? __longlong_as_double(0x7ff8000000000000ll)
+                                       : 0.0;
 #pragma unroll
                 for (int k = 0; k < K; ++k) {
                     const float t0 = warp_sum(acc[0][k]);
@@ -463,13 +572,16 @@ __global__ void __launch_bounds__(PD_THREADS, fp32_min_blocks(K, MODE, NP))
                     const float tj = warp_sum(acc[NACC - 1][k]);
                     const float tij = warp_sum(wi * acc[NACC - 1][k]);
                     if (lane == (k & 31)) {
-                        slot[k] = (first ? 0.0 : slot[k]) + static_cast<double>(t0);
-                        slot[K + k] = (first ? 0.0 : slot[K + k]) + static_cast<double>(ti);
-                        slot[2 * K + k] = (first ? 0.0 : slot[2 * K + k]) + static_cast<double>(tj);
+                        slot[k] = (first ? 0.0 : slot[k]) + static_cast<double>(t0) + bad;
+                        slot[K + k] = (first ? 0.0 : slot[K + k]) + static_cast<double>(ti) + bad;
+                        slot[2 * K + k] =
+                            (first ? 0.0 : slot[2 * K + k]) + static_cast<double>(tj) + bad;
                         slot[3 * K + k] =
-                            (first ? 0.0 : slot[3 * K + k]) + static_cast<double>(tij);
+                            (first ? 0.0 : slot[3 * K + k]) + static_cast<double>(tij) + bad;
                     }
                 }
+              }
+              __syncthreads();  // every read of buffer b done before it is refilled
             }
         }
         __syncthreads();  // s_qres and s_job are rewritten by the next tile
@@ -902,9 +1014,27 @@ __global__ void pd_ffma2_probe(float *out, int iters, float a, float b) {
 
 // ------------------------------------------------------------ launchers
 template <int K, int MODE, int NP>
+static cudaError_t fp32_smem_attr() {
+    // Above 48 KB of dynamic shared memory needs the opt-in attribute, set
+    // once per device (the occupancy query sets it before any stream capture).
+    static std::atomic<uint64_t> done{0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const uint64_t bit = dev < 64 ? (uint64_t{1} << dev) : 0;
+    if (bit && (done.load() & bit)) return cudaSuccess;
+    const cudaError_t e = cudaFuncSetAttribute(pd_pairs_fp32<K, MODE, NP>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               static_cast<int>(PD_FP32_DYN_SMEM));
+    if (e == cudaSuccess && bit) done.fetch_or(bit);
+    return e;
+}
+template <int K, int MODE, int NP>
 static cudaError_t launch_fp32_t(const PdJob *jobs, const int *n_jobs, const PdReqDev *reqs,
                                  int *counter, int grid, cudaStream_t st) {
-    pd_pairs_fp32<K, MODE, NP><<<grid, PD_THREADS, 0, st>>>(jobs, n_jobs, reqs, counter);
+    cudaError_t e = fp32_smem_attr<K, MODE, NP>();
+    if (e != cudaSuccess) return e;
+    pd_pairs_fp32<K, MODE, NP><<<grid, PD_THREADS, PD_FP32_DYN_SMEM, st>>>(jobs, n_jobs, reqs,
+                                                                           counter);
     return cudaGetLastError();
 }
 template <int K, int MODE>
@@ -916,7 +1046,9 @@ static cudaError_t launch_fp64_t(const PdJob *jobs, const int *n_jobs, const PdR
 template <int K, int MODE, int NP>
 static int occupancy_fp32() {
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, pd_pairs_fp32<K, MODE, NP>, PD_THREADS, 0);
+    if (fp32_smem_attr<K, MODE, NP>() != cudaSuccess) return 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, pd_pairs_fp32<K, MODE, NP>, PD_THREADS,
+                                                  PD_FP32_DYN_SMEM);
     return n;
 }
 template <int K, int MODE>
@@ -973,6 +1105,15 @@ int pairs_blocks_per_sm(int precision, int K_, int NP_, int mode) {
     PD_O32(128, 0, 1) PD_O32(128, 0, 2) PD_O32(128, 0, 4) PD_O32(160, 0, 1) PD_O32(192, 0, 1)
     PD_O32(32, 1, 2) PD_O32(64, 1, 2)
     return 0;
+}
+
+cudaError_t prepare_pair_kernels() {
+    const int shapes[][3] = {{32, 0, 4},  {64, 0, 1},  {64, 0, 2},  {64, 0, 4},
+                             {96, 0, 2},  {128, 0, 1}, {128, 0, 2}, {128, 0, 4},
+                             {160, 0, 1}, {192, 0, 1}, {32, 1, 2},  {64, 1, 2}};
+    for (const auto &sh : shapes)
+        if (pairs_blocks_per_sm(0, sh[0], sh[2], sh[1]) <= 0) return cudaErrorInvalidValue;
+    return cudaSuccess;
 }
 
 cudaError_t launch_centroid(const double *xyz, int64_t n_atoms, int n_frames, double *centroid,

@@ -12,6 +12,10 @@ namespace pd {
 bool valid_q_block(int precision, int K);
 bool valid_shape(int precision, int mode, int K, int NP);
 int pairs_blocks_per_sm(int precision, int K, int NP, int mode);
+// Set the launch attributes of every FP32 pair-kernel shape on the current
+// device (their shared-memory opt-in), so that no later launch — one inside a
+// stream capture included — has to.
+cudaError_t prepare_pair_kernels();
 
 // n_jobs points to the tile count in device memory (read once per CTA).
 cudaError_t launch_pairs(int precision, int K, int NP, int mode, const PdJob *jobs,
