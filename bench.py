@@ -386,7 +386,13 @@ def run_serve(args, ws, rank, local):
 
     torch.cuda.set_device(local)
     stream = synth.request_stream(args.requests, args.rate, seed=4 + rank)
-    reqs = [workloads.stream_request(sr, args.precision) for sr in stream]
+    if args.requests > 500:
+        # long streams: compact sub-globules of a pool instead of one RSA run
+        # per request (same density and size distribution)
+        pool = workloads.GlobulePool()
+        reqs = [workloads.stream_request_pooled(sr, pool, args.precision) for sr in stream]
+    else:
+        reqs = [workloads.stream_request(sr, args.precision) for sr in stream]
     ctx = _lib.Context(local, mem_budget_bytes=int(args.budget_gb * (1 << 30)))
     srv = Server(ctx)
     # warm the kernels and graphs on a few requests
@@ -419,6 +425,8 @@ def run_serve(args, ws, rank, local):
             "warmup": 3, "ms_per_step": 1e3 * wall / len(reqs), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": "stream", "requests": len(reqs), "rate_hz": args.rate,
+                       "structures": "pooled compact sub-globules" if args.requests > 500
+                                     else "one RSA globule per request",
                        "n_atoms": "log-uniform 500-50000", "nq": "uniform 100-1000",
                        "qmax": "uniform 0.3-1.0", "solvent_fraction": 0.7,
                        "budget_gb": args.budget_gb, "precision_form": args.precision},

@@ -190,6 +190,81 @@ int pd_plan_set_profiling(pd_ctx *ctx, pd_plan *plan, int enable);
 int pd_plan_pair_kernel_ms(pd_ctx *ctx, pd_plan *plan, double *total_ms, uint64_t *n_launches);
 void pd_plan_destroy(pd_ctx *ctx, pd_plan *plan);
 
+/* Streamed trajectory averages: the frame loop of trajectory_average
+ * (src/trajectory.rs:198-248) for trajectories too long to hold in one
+ * request, fed frame by frame from any reader (the reference reads XTC files
+ * through its XtcIterator, src/trajectory.rs:36-118). pd_stream_open takes
+ * the topology of `req` (species, tables, q grid, precision; req->xyz,
+ * n_frames and frame_weights are ignored; no lattice sets) and the number of
+ * frames solved per batch. pd_stream_push copies n_frames frames
+ * ([n_frames][N][3] HOST memory, Å) and their weights (NULL = 1) into pinned
+ * batches; each full batch is uploaded on its own stream while the previous
+ * one is solved, and push blocks only while both batch buffers are in use.
+ * pd_stream_finish solves the last partial batch, writes the weighted mean
+ * Σ_f w_f·T_f / Σ_f w_f of the six profiles to out_terms ([6][nq] HOST; may
+ * be NULL) and releases the stream; a weight sum that is zero or not normal
+ * is PD_EINVAL, as in the reference (src/trajectory.rs:234-238). */
+typedef struct pd_stream pd_stream;
+int pd_stream_open(pd_ctx *ctx, const pd_request *req, uint32_t frames_per_batch,
+                   pd_stream **out);
+int pd_stream_push(pd_ctx *ctx, pd_stream *s, const double *xyz, const double *weights,
+                   uint64_t n_frames);
+int pd_stream_finish(pd_ctx *ctx, pd_stream *s, double *out_terms);
+
+/* Direct transform of a periodic box (the reference's DirectTransform,
+ * src/explicit.rs:138-147 and :208-230, and the amplitude part of its
+ * DirectModel, :296-325): for each explicit q-vector q_v (Å⁻¹; the
+ * reference's 2π·n/L for integer n), the amplitude
+ * A(q_v) = Σ_j w_j·f_{kind_j}(|q_v|)·e^{i q_v·r_j} over n_points points, and the
+ * self term Σ_m |F_m(q_v)|² over n_molecules equal contiguous molecules
+ * (0 or 1: the whole box; n_points must be a multiple). ff is
+ * [n_kinds][n_vectors]: each kind's form factor at each vector's |q|, as the
+ * host evaluates it (eval_atom_form_factors, src/explicit.rs:360-370). FP64
+ * throughout, one sincos per (vector, point). out is [n_vectors][4]:
+ * Re A, Im A, |A|², Σ_m |F_m|². Blocking; HOST buffers. */
+typedef struct pd_direct_request {
+    uint64_t n_points;         /* >= 1 */
+    const double *xyz;         /* [n_points][3] Å */
+    const uint32_t *kind;      /* [n_points], each < n_kinds */
+    uint32_t n_kinds;          /* >= 1 */
+    uint32_t reserved;         /* must be 0 */
+    const double *ff;          /* [n_kinds][n_vectors] */
+    uint64_t n_vectors;        /* >= 1 */
+    const double *qvec;        /* [n_vectors][3] Å⁻¹ */
+    uint64_t n_molecules;      /* 0 or 1 = whole box, else divides n_points */
+    const double *weight;      /* [n_points] factor on each point's form factor, or NULL
+                                  (DummySet::Weighted, src/solvent/mod.rs:365-371) */
+} pd_direct_request;
+int pd_direct(pd_ctx *ctx, const pd_direct_request *req, double *out);
+
+/* Form factors evaluated on the device: the reference's FormFactor kinds
+ * (src/formfactor.rs:130-201; United is a 101-point Table after loading,
+ * :642-698) on the uniform grid q_k = qmin + (qmax-qmin)·k/max(nq-1, 1),
+ * FP64:
+ *   PD_FF_CONSTANT        c                          params = [c]
+ *   PD_FF_GAUSSIAN        Σ a_i·exp(-b_i·s²) + c, s² = q²/(16π²)
+ *                                                    params = [c, a_0, b_0, …], n = pairs
+ *   PD_FF_SINGLE_GAUSSIAN a·exp(-b·q²)               params = [a, b]
+ *   PD_FF_POLYNOMIAL      Σ c_i·q^i                  params = [c_0 … c_{n-1}]
+ *   PD_FF_TABLE           linear interpolation, exact hit returns the value
+ *                                                    params = [x_0 … x_{n-1}, y_0 … y_{n-1}]
+ * A grid point outside [qlo, qhi] of a form factor is the reference's
+ * QOutOfRange (src/formfactor.rs:191-193): PD_EINVAL, naming it. out is
+ * [n_ff][nq] HOST memory. Blocking. */
+#define PD_FF_CONSTANT 0
+#define PD_FF_GAUSSIAN 1
+#define PD_FF_SINGLE_GAUSSIAN 2
+#define PD_FF_POLYNOMIAL 3
+#define PD_FF_TABLE 4
+typedef struct pd_formfactor {
+    uint32_t type;          /* PD_FF_* */
+    uint32_t n;             /* Gaussian pairs, polynomial coefficients or table points */
+    double qlo, qhi;        /* valid q range, inclusive */
+    const double *params;   /* as listed above */
+} pd_formfactor;
+int pd_formfactor_tables(pd_ctx *ctx, const pd_formfactor *ff, uint32_t n_ff, double qmin,
+                         double qmax, uint64_t nq, double *out);
+
 /* Continuous-batching request loop. pd_submit copies the request, queues it
  * for admission (admitted when device memory within the budget frees up) and
  * returns a ticket at once; its tiles then run interleaved with those of the

@@ -20,6 +20,9 @@
  *   fraser_form_factor    src/solvent/fraser.rs:48-57 (+ SingleGaussian eval
  *                         src/formfactor.rs:196)
  *   SASA shell weight     src/solvent/sasa.rs:54-59
+ *   Direct transform rows  src/explicit.rs:138-147 (complex_amplitude),
+ *                         :208-230 (vacuum_rows: per-molecule F_m, |Σ F_m|²,
+ *                         Σ |F_m|²)
  *   build_model with dummies at their own positions (grid / Voronoi /
  *   caller-supplied DummySets): src/debye.rs:83-130 with
  *   DummySet::form_factors_at src/solvent/mod.rs:357-374
@@ -349,6 +352,42 @@ int pdo_vacuum(size_t n, const double *xyz, const uint32_t *species, const doubl
     int rc = pdo_run(&jb, n_threads);
     free(qv);
     return rc;
+}
+
+/*
+ * Direct transform rows (src/explicit.rs:208-230 with complex_amplitude,
+ * :138-147): for q-vector v, the box is cut into n_mol contiguous molecules of
+ * n/n_mol points; each molecule's amplitude F_m is folded point by point as
+ * (re + f·cos(q·r), im + f·sin(q·r)) with q·r = q_x·x + q_y·y + q_z·z (the
+ * nalgebra dot order); a = Σ_m F_m, self = Σ_m |F_m|². ff is
+ * [n_kinds][n_vec] (each kind at |q_v|). out[v] = (Re a, Im a, |a|², self).
+ */
+void pdo_direct_rows(size_t n, const double *xyz, const uint32_t *kind, const double *weight,
+                     const double *ff, size_t n_vec, const double *qvec, size_t n_mol,
+                     double *out) {
+    const size_t m = n_mol ? n / n_mol : n;
+    for (size_t v = 0; v < n_vec; ++v) {
+        const double qx = qvec[3 * v], qy = qvec[3 * v + 1], qz = qvec[3 * v + 2];
+        double ar = 0.0, ai = 0.0, self = 0.0;
+        for (size_t p0 = 0; p0 < n; p0 += (m ? m : 1)) {
+            double re = 0.0, im = 0.0;
+            for (size_t p = p0; p < p0 + m && p < n; ++p) {
+                /* DummySet::form_factors_at: w·F for weighted sets */
+                const double f = weight ? weight[p] * ff[(size_t)kind[p] * n_vec + v]
+                                        : ff[(size_t)kind[p] * n_vec + v];
+                const double qr = qx * xyz[3 * p] + qy * xyz[3 * p + 1] + qz * xyz[3 * p + 2];
+                re = re + f * cos(qr);
+                im = im + f * sin(qr);
+            }
+            ar += re;
+            ai += im;
+            self += re * re + im * im;
+        }
+        out[4 * v] = ar;
+        out[4 * v + 1] = ai;
+        out[4 * v + 2] = ar * ar + ai * ai;
+        out[4 * v + 3] = self;
+    }
 }
 
 /* ---- form factors (host-side inputs of the path) ---- */

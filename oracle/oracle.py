@@ -52,6 +52,9 @@ def lib():
         L.pdo_build_model_sets.argtypes = [C.c_size_t, _D, _U32, _D, C.c_size_t, _D, _U32, _D,
                                            C.c_size_t, _D, _D, _D, C.c_double, C.c_double,
                                            C.c_size_t, _U32, C.c_size_t, C.c_int, C.c_int, _D]
+        L.pdo_direct_rows.restype = None
+        L.pdo_direct_rows.argtypes = [C.c_size_t, _D, _U32, _D, _D, C.c_size_t, _D, C.c_size_t,
+                                      _D]
         L.pdo_vacuum.restype = C.c_int
         L.pdo_vacuum.argtypes = [C.c_size_t, _D, _U32, _D, C.c_double, C.c_double, C.c_size_t,
                                  _U32, C.c_size_t, C.c_int, C.c_int, _D]
@@ -148,6 +151,20 @@ def build_model_sets(xyz, species, ff_atoms, exc_xyz=None, exc_kind=None, ff_exc
         _d(out))
     if rc != 0:
         raise MemoryError("oracle allocation failed")
+    return out
+
+
+def direct_rows(xyz, kind, ff, qvec, n_molecules=1, weight=None) -> np.ndarray:
+    """[n_vec, 4] = (Re A, Im A, |A|², Σ_m |F_m|²) per q-vector
+    (src/explicit.rs:208-230)."""
+    xyz = _c(xyz).reshape(-1, 3)
+    kind = _c(kind, np.uint32)
+    ff = _c(ff)
+    qvec = _c(qvec).reshape(-1, 3)
+    out = np.empty((len(qvec), 4))
+    lib().pdo_direct_rows(len(kind), _d(xyz), kind.ctypes.data_as(_U32),
+                          _d(None if weight is None else _c(weight)), _d(ff), len(qvec),
+                          _d(qvec), int(n_molecules), _d(out))
     return out
 
 

@@ -42,6 +42,31 @@ class PdLattice(C.Structure):
     ]
 
 
+class PdFormFactor(C.Structure):
+    _fields_ = [
+        ("type", C.c_uint32),
+        ("n", C.c_uint32),
+        ("qlo", C.c_double),
+        ("qhi", C.c_double),
+        ("params", C.POINTER(C.c_double)),
+    ]
+
+
+class PdDirectRequest(C.Structure):
+    _fields_ = [
+        ("n_points", C.c_uint64),
+        ("xyz", C.POINTER(C.c_double)),
+        ("kind", C.POINTER(C.c_uint32)),
+        ("n_kinds", C.c_uint32),
+        ("reserved", C.c_uint32),
+        ("ff", C.POINTER(C.c_double)),
+        ("n_vectors", C.c_uint64),
+        ("qvec", C.POINTER(C.c_double)),
+        ("n_molecules", C.c_uint64),
+        ("weight", C.POINTER(C.c_double)),
+    ]
+
+
 class PdRequest(C.Structure):
     _fields_ = [
         ("n_atoms", C.c_uint64),
@@ -100,6 +125,12 @@ SIGNATURES = {
     "pd_measure_fp32_peak": (C.c_int, [_P, _D, _D]),
     "pd_launch_count": (C.c_uint64, [_P]),
     "pd_solve_noalloc": (C.c_int, [C.POINTER(PdRequest), C.c_void_p, C.c_void_p, C.c_void_p]),
+    "pd_direct": (C.c_int, [_P, C.POINTER(PdDirectRequest), _D]),
+    "pd_formfactor_tables": (C.c_int, [_P, C.POINTER(PdFormFactor), C.c_uint32, C.c_double,
+                                       C.c_double, C.c_uint64, _D]),
+    "pd_stream_open": (C.c_int, [_P, C.POINTER(PdRequest), C.c_uint32, C.POINTER(_P)]),
+    "pd_stream_push": (C.c_int, [_P, _P, _D, _D, C.c_uint64]),
+    "pd_stream_finish": (C.c_int, [_P, _P, _D]),
 }
 
 # Size of the fixed device scratch behind pd_solve_noalloc.

@@ -220,6 +220,9 @@ struct DevPlan {
     // Tile share of a multi-GPU solve: the tiles in the device job list are
     // this rank's; rank 0 adds the i = j terms and the exact q = 0 sums.
     uint32_t rank = 0, world = 1;
+    // Finish with the unnormalised frame sum Σ_f w_f·T_f instead of the mean
+    // (streamed trajectories add batches before dividing once).
+    bool frame_sum = false;
     template <class T>
     T *dptr(uint64_t off) const {
         return reinterpret_cast<T *>(base + off);
@@ -413,7 +416,7 @@ int finish_devplan(pd_ctx *ctx, DevPlan &dp, double *out_dev, cudaStream_t st) {
     double *dst = out_dev ? out_dev : dp.dptr<double>(L.out);
     if (P.n_frames > 1) {
         PD_CUDA(ctx, pd::launch_frame_mean(dp.dptr<double>(L.terms), dp.dptr<double>(L.fw),
-                                           P.n_frames, P.nq, dst, st));
+                                           P.n_frames, P.nq, dst, st, !dp.frame_sum));
         ctx->launches += 1;
     } else {
         PD_CUDA(ctx, cudaMemcpyAsync(dst, dp.dptr<double>(L.terms),
@@ -1537,6 +1540,407 @@ int pd_measure_fp32_peak(pd_ctx *ctx, double *tflops_ffma, double *tflops_ffma2)
 uint64_t pd_launch_count(pd_ctx *ctx) { return ctx ? ctx->launches.load() : 0; }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------- direct transform
+extern "C" int pd_direct(pd_ctx *ctx, const pd_direct_request *req, double *out) {
+    if (!ctx || !req || !out) return PD_EINVAL;
+    const uint64_t n = req->n_points, nv = req->n_vectors;
+    const uint64_t nm = req->n_molecules ? req->n_molecules : 1;
+    std::string msg;
+    if (n == 0 || nv == 0 || req->n_kinds == 0 || !req->xyz || !req->kind || !req->ff ||
+        !req->qvec || req->reserved)
+        msg = "pd_direct: n_points, n_vectors, n_kinds >= 1 and xyz, kind, ff, qvec required";
+    else if (n > (1ull << 30) || nv > (1ull << 26))
+        msg = "pd_direct: n_points <= 2^30 and n_vectors <= 2^26";
+    else if (n % nm)
+        msg = "box point count (" + std::to_string(n) + ") is not a multiple of the molecule "
+              "count (" + std::to_string(nm) + ")";
+    if (msg.empty()) {
+        for (uint64_t i = 0; i < n; ++i)
+            if (req->kind[i] >= req->n_kinds) {
+                msg = "kind " + std::to_string(req->kind[i]) + " at point " + std::to_string(i) +
+                      " is >= n_kinds";
+                break;
+            }
+        for (uint64_t i = 0; msg.empty() && i < 3 * n; ++i)
+            if (!std::isfinite(req->xyz[i])) msg = "non-finite coordinate";
+        for (uint64_t i = 0; msg.empty() && i < 3 * nv; ++i)
+            if (!std::isfinite(req->qvec[i])) msg = "non-finite q-vector";
+        for (uint64_t i = 0; msg.empty() && i < nv * req->n_kinds; ++i)
+            if (!std::isfinite(req->ff[i])) msg = "non-finite form factor";
+        for (uint64_t i = 0; msg.empty() && req->weight && i < n; ++i)
+            if (!std::isfinite(req->weight[i])) msg = "non-finite point weight";
+    }
+    if (!msg.empty()) {
+        ctx->set_error(msg);
+        return PD_EINVAL;
+    }
+    const int64_t mol = static_cast<int64_t>(n / nm);
+    const int64_t chunks = pd::direct_chunks(static_cast<int64_t>(n), mol);
+    if (chunks > 65535) {
+        ctx->set_error("pd_direct: too many point chunks for one launch");
+        return PD_EINVAL;
+    }
+    std::lock_guard<std::mutex> g(ctx->solve_mu);
+    cudaSetDevice(ctx->device);
+    cudaStream_t st = ctx->stream;
+    const size_t b_xyz = n * 24, b_kind = n * 4, b_ff = nv * req->n_kinds * 8, b_q = nv * 24,
+                 b_part = static_cast<size_t>(chunks) * nv * 40, b_out = nv * 32,
+                 b_w = req->weight ? n * 8 : 0;
+    const size_t total = align_up(b_xyz, 256) + align_up(b_kind, 256) + align_up(b_ff, 256) +
+                         align_up(b_q, 256) + align_up(b_part, 256) + align_up(b_w, 256) + b_out;
+    char *base = nullptr;
+    PD_CUDA(ctx, cudaMallocFromPoolAsync(reinterpret_cast<void **>(&base), total, ctx->pool, st));
+    char *cur = base;
+    auto take = [&](size_t bytes) {
+        char *r = cur;
+        cur += align_up(bytes, 256);
+        return r;
+    };
+    double *d_xyz = reinterpret_cast<double *>(take(b_xyz));
+    uint32_t *d_kind = reinterpret_cast<uint32_t *>(take(b_kind));
+    double *d_ff = reinterpret_cast<double *>(take(b_ff));
+    double *d_q = reinterpret_cast<double *>(take(b_q));
+    double *d_part = reinterpret_cast<double *>(take(b_part));
+    double *d_w = req->weight ? reinterpret_cast<double *>(take(b_w)) : nullptr;
+    double *d_out = reinterpret_cast<double *>(take(b_out));
+    cudaError_t e = cudaMemcpyAsync(d_xyz, req->xyz, b_xyz, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_kind, req->kind, b_kind, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_ff, req->ff, b_ff, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_q, req->qvec, b_q, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && d_w)
+        e = cudaMemcpyAsync(d_w, req->weight, b_w, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+        e = pd::launch_direct(d_xyz, d_kind, d_w, d_ff, d_q, static_cast<int64_t>(nv),
+                              static_cast<int64_t>(n), mol, d_part, chunks, d_out, st);
+    if (e == cudaSuccess) {
+        ctx->launches += 2;
+        e = cudaMemcpyAsync(out, d_out, b_out, cudaMemcpyDeviceToHost, st);
+    }
+    cudaFreeAsync(base, st);
+    const cudaError_t e2 = cudaStreamSynchronize(st);
+    if (e == cudaSuccess) e = e2;
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "pd_direct");
+    return PD_OK;
+}
+
+// ---------------------------------------------------------------- form factors
+extern "C" int pd_formfactor_tables(pd_ctx *ctx, const pd_formfactor *ff, uint32_t n_ff,
+                                    double qmin, double qmax, uint64_t nq, double *out) {
+    if (!ctx || !ff || !out || n_ff == 0 || nq == 0 || nq > (1ull << 24)) return PD_EINVAL;
+    if (!std::isfinite(qmin) || !std::isfinite(qmax) || qmin < 0.0 || qmax < qmin) {
+        ctx->set_error("q range must satisfy 0 <= qmin <= qmax (finite)");
+        return PD_EINVAL;
+    }
+    std::vector<int32_t> desc(3 * n_ff);
+    std::vector<double> range(2 * n_ff), params;
+    for (uint32_t f = 0; f < n_ff; ++f) {
+        const pd_formfactor &d = ff[f];
+        size_t np = 0;
+        bool ok = d.params != nullptr && !(d.qlo > d.qhi) && !std::isnan(d.qlo) &&
+                  !std::isnan(d.qhi);
+        switch (d.type) {
+            case PD_FF_CONSTANT: np = 1; break;
+            case PD_FF_GAUSSIAN: np = 1 + 2 * static_cast<size_t>(d.n); break;
+            case PD_FF_SINGLE_GAUSSIAN: np = 2; break;
+            case PD_FF_POLYNOMIAL: np = d.n; ok = ok && d.n >= 1; break;
+            case PD_FF_TABLE: np = 2 * static_cast<size_t>(d.n); ok = ok && d.n >= 2; break;
+            default: ok = false;
+        }
+        if (ok && d.n > 4096) ok = false;
+        for (size_t i = 0; ok && i < np; ++i) ok = std::isfinite(d.params[i]);
+        if (ok && d.type == PD_FF_TABLE)
+            for (uint32_t i = 1; ok && i < d.n; ++i) ok = d.params[i] > d.params[i - 1];
+        if (!ok) {
+            ctx->set_error("form factor " + std::to_string(f) +
+                           ": unknown type, bad parameters or range (tables need >= 2 "
+                           "increasing points)");
+            return PD_EINVAL;
+        }
+        desc[3 * f] = static_cast<int32_t>(d.type);
+        desc[3 * f + 1] = static_cast<int32_t>(d.n);
+        desc[3 * f + 2] = static_cast<int32_t>(params.size());
+        range[2 * f] = d.qlo;
+        range[2 * f + 1] = d.qhi;
+        params.insert(params.end(), d.params, d.params + np);
+    }
+    if (params.size() > (1u << 26)) return PD_EINVAL;
+    params.push_back(0.0);
+    std::lock_guard<std::mutex> g(ctx->solve_mu);
+    cudaSetDevice(ctx->device);
+    cudaStream_t st = ctx->stream;
+    const size_t b_desc = desc.size() * 4, b_range = range.size() * 8,
+                 b_par = params.size() * 8, b_out = static_cast<size_t>(n_ff) * nq * 8;
+    const size_t total = align_up(b_desc, 256) + align_up(b_range, 256) + align_up(b_par, 256) +
+                         align_up(4, 256) + b_out;
+    char *base = nullptr;
+    PD_CUDA(ctx, cudaMallocFromPoolAsync(reinterpret_cast<void **>(&base), total, ctx->pool, st));
+    char *cur = base;
+    auto take = [&](size_t bytes) {
+        char *r = cur;
+        cur += align_up(bytes, 256);
+        return r;
+    };
+    int32_t *d_desc = reinterpret_cast<int32_t *>(take(b_desc));
+    double *d_range = reinterpret_cast<double *>(take(b_range));
+    double *d_par = reinterpret_cast<double *>(take(b_par));
+    int *d_bad = reinterpret_cast<int *>(take(4));
+    double *d_out = reinterpret_cast<double *>(take(b_out));
+    int bad = 0;
+    cudaError_t e = cudaMemcpyAsync(d_desc, desc.data(), b_desc, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_range, range.data(), b_range, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_par, params.data(), b_par, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_bad, 0, 4, st);
+    if (e == cudaSuccess)
+        e = pd::launch_ff_eval(d_desc, d_range, d_par, static_cast<int32_t>(n_ff), qmin, qmax,
+                               static_cast<int64_t>(nq), d_bad, d_out, st);
+    if (e == cudaSuccess) {
+        ctx->launches += 1;
+        e = cudaMemcpyAsync(out, d_out, b_out, cudaMemcpyDeviceToHost, st);
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&bad, d_bad, 4, cudaMemcpyDeviceToHost, st);
+    cudaFreeAsync(base, st);
+    const cudaError_t e2 = cudaStreamSynchronize(st);
+    if (e == cudaSuccess) e = e2;
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "pd_formfactor_tables");
+    if (bad) {
+        const pd_formfactor &d = ff[bad - 1];
+        ctx->set_error("q outside the range [" + std::to_string(d.qlo) + ", " +
+                       std::to_string(d.qhi) + "] of form factor " + std::to_string(bad - 1) +
+                       " (QOutOfRange)");
+        return PD_EINVAL;
+    }
+    return PD_OK;
+}
+
+// ---------------------------------------------------------------- streamed trajectories
+// A trajectory average fed frame by frame: frames are assembled in pinned
+// batches of B frames, each batch is uploaded on its own stream while the
+// previous batch is solved, and every batch adds its unnormalised
+// Σ_f w_f·T_f to an FP64 accumulator (batches in submission order); finish
+// divides once by Σ w_f, as the reference's frame loop does
+// (src/trajectory.rs:198-248).
+struct pd_stream {
+    DevPlan dp;
+    uint32_t B = 0;
+    uint64_t frame_doubles = 0;       // 3·N
+    cudaStream_t cs = nullptr, us = nullptr;  // compute, upload
+    double *d_xyz[2] = {nullptr, nullptr};
+    double *h_xyz[2] = {nullptr, nullptr};
+    double *h_w[2] = {nullptr, nullptr};
+    cudaEvent_t uploaded[2] = {nullptr, nullptr}, computed[2] = {nullptr, nullptr};
+    bool pending[2] = {false, false};
+    int cur = 0;
+    uint32_t fill = 0;
+    double *d_acc = nullptr, *d_batch = nullptr;
+    double wsum = 0.0;
+    uint64_t frames = 0;
+    bool failed = false;
+};
+
+namespace {
+
+void stream_free(pd_ctx *ctx, pd_stream *s) {
+    if (s->cs) cudaStreamSynchronize(s->cs);
+    if (s->us) cudaStreamSynchronize(s->us);
+    for (int b = 0; b < 2; ++b) {
+        if (s->d_xyz[b]) cudaFree(s->d_xyz[b]);
+        if (s->h_xyz[b]) cudaFreeHost(s->h_xyz[b]);
+        if (s->h_w[b]) cudaFreeHost(s->h_w[b]);
+        if (s->uploaded[b]) cudaEventDestroy(s->uploaded[b]);
+        if (s->computed[b]) cudaEventDestroy(s->computed[b]);
+    }
+    if (s->d_acc) cudaFree(s->d_acc);
+    if (s->d_batch) cudaFree(s->d_batch);
+    free_devplan(ctx, s->dp, s->cs ? s->cs : ctx->stream);
+    if (s->cs) cudaStreamSynchronize(s->cs);
+    if (s->cs) cudaStreamDestroy(s->cs);
+    if (s->us) cudaStreamDestroy(s->us);
+    delete s;
+}
+
+// Upload and solve the frames assembled in host buffer s->cur.
+int stream_submit(pd_ctx *ctx, pd_stream *s) {
+    const int b = s->cur;
+    const uint32_t n = s->fill;
+    if (n == 0) return PD_OK;
+    const size_t fb = s->frame_doubles * 8;
+    // pad a partial batch with copies of its first frame at weight 0
+    double wb = 0.0;
+    for (uint32_t f = 0; f < n; ++f) wb += s->h_w[b][f];
+    for (uint32_t f = n; f < s->B; ++f) {
+        std::memcpy(s->h_xyz[b] + f * s->frame_doubles, s->h_xyz[b], fb);
+        s->h_w[b][f] = 0.0;
+    }
+    // device buffer b was last read by the batch that recorded computed[b]
+    if (s->pending[b]) PD_CUDA(ctx, cudaStreamWaitEvent(s->us, s->computed[b], 0));
+    PD_CUDA(ctx, cudaMemcpyAsync(s->d_xyz[b], s->h_xyz[b], fb * s->B, cudaMemcpyHostToDevice,
+                                 s->us));
+    PD_CUDA(ctx, cudaEventRecord(s->uploaded[b], s->us));
+    PD_CUDA(ctx, cudaStreamWaitEvent(s->cs, s->uploaded[b], 0));
+    const Layout &L = s->dp.L;
+    PD_CUDA(ctx, cudaMemcpyAsync(s->dp.dptr<double>(L.fw), s->h_w[b], 8ull * s->B,
+                                 cudaMemcpyHostToDevice, s->cs));
+    s->dp.xyz_dev = s->d_xyz[b];
+    int rc = run_devplan(ctx, s->dp, s->d_batch, s->cs);
+    if (rc) return rc;
+    // one-frame plans finish with the frame's terms: weight them here
+    const double scale = s->B == 1 ? s->h_w[b][0] : 1.0;
+    PD_CUDA(ctx, pd::launch_stream_accumulate(s->d_batch, scale, 6 * s->dp.P.nq, s->d_acc, s->cs));
+    ctx->launches += 1;
+    PD_CUDA(ctx, cudaEventRecord(s->computed[b], s->cs));
+    s->pending[b] = true;
+    s->wsum += wb;
+    s->frames += n;
+    s->cur ^= 1;
+    s->fill = 0;
+    return PD_OK;
+}
+
+}  // namespace
+
+extern "C" int pd_stream_open(pd_ctx *ctx, const pd_request *req, uint32_t frames_per_batch,
+                              pd_stream **out) {
+    if (!ctx || !req || !out || frames_per_batch == 0 || frames_per_batch > 4096) return PD_EINVAL;
+    *out = nullptr;
+    pd_request r = *req;
+    std::vector<double> dummy;
+    if (r.n_atoms == 0) {
+        ctx->set_error("n_atoms must be >= 1");
+        return PD_EINVAL;
+    }
+    if (r.n_lattices) {
+        ctx->set_error("streamed trajectories take atoms only (lattice sets need one frame)");
+        return PD_EINVAL;
+    }
+    r.n_frames = frames_per_batch;
+    r.frame_weights = nullptr;
+    dummy.assign(static_cast<size_t>(r.n_atoms) * 3 * frames_per_batch, 0.0);
+    r.xyz = dummy.data();
+    std::string msg;
+    int rc = pd::validate_request(&r, false, msg);
+    if (rc) {
+        ctx->set_error(msg);
+        return rc;
+    }
+    std::lock_guard<std::mutex> g(ctx->solve_mu);
+    cudaSetDevice(ctx->device);
+    auto *s = new pd_stream();
+    s->B = frames_per_batch;
+    s->frame_doubles = static_cast<uint64_t>(r.n_atoms) * 3;
+    s->dp.frame_sum = true;
+    cudaError_t e = cudaStreamCreateWithFlags(&s->cs, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->us, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        stream_free(ctx, s);
+        return cuda_fail(ctx, e, "pd_stream_open: streams");
+    }
+    rc = create_devplan(ctx, &r, r.species, r.hyd_weights, false, s->dp, s->cs);
+    if (rc) {
+        stream_free(ctx, s);
+        return rc;
+    }
+    const size_t fb = s->frame_doubles * 8 * s->B;
+    const size_t nq6 = 6ull * r.nq * 8;
+    for (int b = 0; b < 2 && e == cudaSuccess; ++b) {
+        e = cudaMalloc(reinterpret_cast<void **>(&s->d_xyz[b]), fb);
+        if (e == cudaSuccess) e = cudaHostAlloc(reinterpret_cast<void **>(&s->h_xyz[b]), fb, 0);
+        if (e == cudaSuccess) e = cudaHostAlloc(reinterpret_cast<void **>(&s->h_w[b]), 8ull * s->B, 0);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->uploaded[b], cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->computed[b], cudaEventDisableTiming);
+    }
+    if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void **>(&s->d_acc), nq6);
+    if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void **>(&s->d_batch), nq6);
+    if (e == cudaSuccess) e = cudaMemsetAsync(s->d_acc, 0, nq6, s->cs);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->cs);
+    if (e != cudaSuccess) {
+        stream_free(ctx, s);
+        return cuda_fail(ctx, e, "pd_stream_open: buffers");
+    }
+    *out = s;
+    return PD_OK;
+}
+
+extern "C" int pd_stream_push(pd_ctx *ctx, pd_stream *s, const double *xyz,
+                              const double *weights, uint64_t n_frames) {
+    if (!ctx || !s || (!xyz && n_frames)) return PD_EINVAL;
+    if (s->failed) {
+        ctx->set_error("the stream failed earlier");
+        return PD_EDEVICE;
+    }
+    for (uint64_t i = 0; i < n_frames * s->frame_doubles; ++i)
+        if (!std::isfinite(xyz[i])) {
+            ctx->set_error("non-finite coordinate at index " + std::to_string(i));
+            return PD_EINVAL;
+        }
+    for (uint64_t f = 0; weights && f < n_frames; ++f)
+        if (!std::isfinite(weights[f])) {
+            ctx->set_error("non-finite frame weight");
+            return PD_EINVAL;
+        }
+    std::lock_guard<std::mutex> g(ctx->solve_mu);
+    cudaSetDevice(ctx->device);
+    for (uint64_t f = 0; f < n_frames; ++f) {
+        const int b = s->cur;
+        if (s->fill == 0 && s->pending[b]) {  // host buffer b is read until its batch is done
+            cudaError_t e = cudaEventSynchronize(s->computed[b]);
+            if (e != cudaSuccess) {
+                s->failed = true;
+                return cuda_fail(ctx, e, "pd_stream_push");
+            }
+        }
+        std::memcpy(s->h_xyz[b] + s->fill * s->frame_doubles, xyz + f * s->frame_doubles,
+                    s->frame_doubles * 8);
+        s->h_w[b][s->fill] = weights ? weights[f] : 1.0;
+        if (++s->fill == s->B) {
+            int rc = stream_submit(ctx, s);
+            if (rc) {
+                s->failed = true;
+                return rc;
+            }
+        }
+    }
+    return PD_OK;
+}
+
+extern "C" int pd_stream_finish(pd_ctx *ctx, pd_stream *s, double *out_terms) {
+    if (!ctx || !s) return PD_EINVAL;
+    int rc = PD_OK;
+    {
+        std::lock_guard<std::mutex> g(ctx->solve_mu);
+        cudaSetDevice(ctx->device);
+        if (!s->failed) rc = stream_submit(ctx, s);
+        const size_t n6 = 6ull * s->dp.P.nq;
+        std::vector<double> acc(n6);
+        if (rc == PD_OK && !s->failed) {
+            cudaError_t e = cudaMemcpyAsync(acc.data(), s->d_acc, n6 * 8, cudaMemcpyDeviceToHost, s->cs);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(s->cs);
+            if (e != cudaSuccess) rc = cuda_fail(ctx, e, "pd_stream_finish");
+        } else if (rc == PD_OK) {
+            ctx->set_error("the stream failed earlier");
+            rc = PD_EDEVICE;
+        }
+        if (rc == PD_OK && s->frames == 0) {
+            ctx->set_error("no frames were pushed");
+            rc = PD_EINVAL;
+        }
+        // trajectory_average rejects a weight sum that is zero or not normal
+        // (src/trajectory.rs:234-238)
+        if (rc == PD_OK && !std::isnormal(std::fabs(s->wsum))) {
+            ctx->set_error("weights of the " + std::to_string(s->frames) +
+                           " averaged frames sum to " + std::to_string(s->wsum) +
+                           "; cannot normalize");
+            rc = PD_EINVAL;
+        }
+        if (rc == PD_OK && out_terms)
+            for (size_t t = 0; t < n6; ++t) out_terms[t] = acc[t] / s->wsum;
+    }
+    std::lock_guard<std::mutex> g(ctx->solve_mu);
+    cudaSetDevice(ctx->device);
+    stream_free(ctx, s);
+    return rc;
+}
+
 
 // ------------------------------------------------ allocation-free solve
 // pd_solve_noalloc runs the same pipeline as a plan execution, but every

@@ -26,6 +26,7 @@
 
 #include "pd_common.h"
 #include "pd_kernels.h"
+#include "pripps_debye.h"
 
 namespace pd {
 
@@ -950,7 +951,8 @@ __global__ void __launch_bounds__(256) pd_lattice_sums(const unsigned long long 
 
 // Frame-weighted mean of the six profiles, frames added in order.
 __global__ void pd_frame_mean(const double *__restrict__ terms, const double *__restrict__ fw,
-                              int32_t n_frames, int32_t nq, double *__restrict__ out) {
+                              int32_t n_frames, int32_t nq, int32_t normalize,
+                              double *__restrict__ out) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= 6 * nq) return;
     double s = 0.0, wsum = 0.0;
@@ -959,7 +961,175 @@ __global__ void pd_frame_mean(const double *__restrict__ terms, const double *__
         s += w * terms[static_cast<int64_t>(f) * 6 * nq + t];
         wsum += w;
     }
-    out[t] = s / wsum;
+    out[t] = normalize ? s / wsum : s;
+}
+
+// Streamed trajectories: acc += batch, where batch is one batch's
+// unnormalised Σ_f w_f·T_f (or, for a one-frame batch, T times its weight).
+// Batches are added in submission order.
+__global__ void pd_stream_accumulate(const double *__restrict__ batch, double scale, int32_t n,
+                                     double *__restrict__ acc) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) acc[t] += scale * batch[t];
+}
+
+// ------------------------------------------------------------ Direct transform
+// Amplitudes of a periodic box at explicit q-vectors (the reference's
+// DirectTransform, src/explicit.rs:138-147 and :208-230), FP64 throughout:
+// F(q) = Σ_j f_j(q)·e^{i q·r_j} with q·r evaluated as q_x·x + q_y·y + q_z·z and
+// one sincos per (vector, point). The points are split into chunks that never
+// straddle a molecule: groups of whole molecules (molecules of at most
+// PD_DIRECT_CHUNK points), for which the chunk also forms Σ_m |F_m|², or
+// slices of PD_DIRECT_CHUNK points of one molecule (the last one shorter),
+// whose partial amplitudes the reduction joins per molecule. One thread per
+// q-vector; the chunk's points are read as warp-uniform broadcasts.
+constexpr int PD_DIRECT_CHUNK = 1024;
+
+__global__ void __launch_bounds__(128) pd_direct_chunks(const double *__restrict__ xyz,
+                                                        const uint32_t *__restrict__ kind,
+                                                        const double *__restrict__ weight,
+                                                        const double *__restrict__ ff,
+                                                        const double *__restrict__ qvec,
+                                                        int64_t n_vec, int64_t mol_size,
+                                                        int64_t chunk_points,
+                                                        int64_t slices_per_mol,
+                                                        int64_t n_points,
+                                                        double *__restrict__ part) {
+    const int64_t v = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    const int64_t c = blockIdx.y;
+    if (v >= n_vec) return;
+    const double qx = qvec[3 * v], qy = qvec[3 * v + 1], qz = qvec[3 * v + 2];
+    int64_t p0, p1;
+    if (slices_per_mol == 1) {  // whole molecules
+        p0 = c * chunk_points;
+        p1 = min(n_points, p0 + chunk_points);
+    } else {                    // slice s of molecule m
+        const int64_t m = c / slices_per_mol, sl = c % slices_per_mol;
+        p0 = m * mol_size + sl * chunk_points;
+        p1 = min((m + 1) * mol_size, p0 + chunk_points);
+    }
+    const bool whole = slices_per_mol == 1;
+    double ar = 0.0, ai = 0.0, fr = 0.0, fi = 0.0, self = 0.0;
+    for (int64_t p = p0; p < p1; ++p) {
+        const double x = xyz[3 * p], y = xyz[3 * p + 1], z = xyz[3 * p + 2];
+        double f = ff[static_cast<int64_t>(kind[p]) * n_vec + v];
+        if (weight) f = weight[p] * f;  // DummySet::Weighted: w·F
+        const double qr = qx * x + qy * y + qz * z;
+        double sn, cs;
+        sincos(qr, &sn, &cs);
+        fr += f * cs;
+        fi += f * sn;
+        if (whole && (p + 1) % mol_size == 0) {  // a molecule ends inside this chunk
+            ar += fr;
+            ai += fi;
+            self += fr * fr + fi * fi;
+            fr = 0.0;
+            fi = 0.0;
+        }
+    }
+    // whole molecules: (A, Σ|F_m|²); a slice of a molecule: its open partial F
+    double *o = part + (c * n_vec + v) * 5;
+    o[0] = ar;
+    o[1] = ai;
+    o[2] = self;
+    o[3] = fr;
+    o[4] = fi;
+}
+
+// Per q-vector: A = Σ chunks, Σ_m |F_m|² with the slices of a molecule joined
+// first (chunks in order). out[v] = (Re A, Im A, |A|², Σ_m |F_m|²).
+__global__ void pd_direct_reduce(const double *__restrict__ part, int64_t n_vec, int64_t n_chunks,
+                                 int64_t slices_per_mol, double *__restrict__ out) {
+    const int64_t v = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (v >= n_vec) return;
+    double ar = 0.0, ai = 0.0, self = 0.0, fr = 0.0, fi = 0.0;
+    for (int64_t c = 0; c < n_chunks; ++c) {
+        const double *o = part + (c * n_vec + v) * 5;
+        ar += o[0];
+        ai += o[1];
+        self += o[2];
+        if (slices_per_mol > 1) {
+            fr += o[3];
+            fi += o[4];
+            if ((c + 1) % slices_per_mol == 0) {
+                ar += fr;
+                ai += fi;
+                self += fr * fr + fi * fi;
+                fr = 0.0;
+                fi = 0.0;
+            }
+        }
+    }
+    out[4 * v] = ar;
+    out[4 * v + 1] = ai;
+    out[4 * v + 2] = ar * ar + ai * ai;
+    out[4 * v + 3] = self;
+}
+
+// ------------------------------------------------------------ form factors
+// One thread per (form factor, grid point): the reference's FormFactor::eval
+// (src/formfactor.rs:188-201) in FP64 on q_k = qmin + (qmax - qmin)·k/denom.
+// Descriptor d: type, n, offset of its parameters in `params`; range [lo, hi].
+// A point outside the range records the form factor's index + 1 in *bad.
+__global__ void pd_ff_eval(const int32_t *__restrict__ desc, const double *__restrict__ range,
+                           const double *__restrict__ params, int32_t n_ff, double qmin,
+                           double qmax, int64_t nq, int *__restrict__ bad,
+                           double *__restrict__ out) {
+    const int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (t >= n_ff * nq) return;
+    const int f = static_cast<int>(t / nq);
+    const int64_t k = t % nq;
+    const double denom = static_cast<double>(nq > 1 ? nq - 1 : 1);
+    const double q = qmin + (qmax - qmin) * static_cast<double>(k) / denom;
+    const int type = desc[3 * f], n = desc[3 * f + 1];
+    const double *p = params + desc[3 * f + 2];
+    double v = 0.0;
+    if (!(range[2 * f] <= q && q <= range[2 * f + 1])) {
+        atomicMax(bad, f + 1);
+    } else if (type == PD_FF_CONSTANT) {
+        v = p[0];
+    } else if (type == PD_FF_GAUSSIAN) {
+        const double PI = 3.14159265358979323846;
+        const double s2 = q * q / (16.0 * PI * PI);
+        double sum = 0.0;
+        for (int i = 0; i < n; ++i) sum += p[1 + 2 * i] * exp(-p[2 + 2 * i] * s2);
+        v = sum + p[0];
+    } else if (type == PD_FF_SINGLE_GAUSSIAN) {
+        v = p[0] * exp(-p[1] * q * q);
+    } else if (type == PD_FF_POLYNOMIAL) {
+        double sum = 0.0;
+        for (int i = 0; i < n; ++i) {
+            double pw = 1.0;
+            for (int e = 0; e < i; ++e) pw *= q;  // q^i by repeated products (Rust powi)
+            sum += p[i] * pw;
+        }
+        v = sum;
+    } else if (type == PD_FF_TABLE) {
+        const double *xs = p, *ys = p + n;
+        int low = 0, high = n - 1;
+        bool hit = false;
+        while (low < high) {
+            const int mid = (low + high) / 2;
+            if (q < xs[mid]) {
+                high = mid;
+            } else if (q > xs[mid]) {
+                low = mid + 1;
+            } else {
+                v = ys[mid];
+                hit = true;
+                break;
+            }
+        }
+        if (!hit) {
+            if (low == 0) {  // q == xs[0] is a hit; below xs[0] is out of range
+                v = ys[0];
+            } else {
+                const double x0 = xs[low - 1], y0 = ys[low - 1], x1 = xs[low], y1 = ys[low];
+                v = y0 + (q - x0) * (y1 - y0) / (x1 - x0);
+            }
+        }
+    }
+    out[t] = v;
 }
 
 // ------------------------------------------------------------ FP32 probe
@@ -1202,9 +1372,62 @@ cudaError_t launch_lattice_sums(const unsigned long long *hist, const PdLatDev *
 }
 
 cudaError_t launch_frame_mean(const double *terms, const double *fw, int32_t n_frames, int32_t nq,
-                              double *out, cudaStream_t st) {
+                              double *out, cudaStream_t st, bool normalize) {
     const int grid = (6 * nq + 127) / 128;
-    pd_frame_mean<<<grid, 128, 0, st>>>(terms, fw, n_frames, nq, out);
+    pd_frame_mean<<<grid, 128, 0, st>>>(terms, fw, n_frames, nq, normalize ? 1 : 0, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_stream_accumulate(const double *batch, double scale, int32_t n, double *acc,
+                                     cudaStream_t st) {
+    pd_stream_accumulate<<<(n + 127) / 128, 128, 0, st>>>(batch, scale, n, acc);
+    return cudaGetLastError();
+}
+
+// Chunking of n_points points in molecules of mol_size: (points per chunk,
+// slices per molecule, number of chunks).
+static void direct_layout(int64_t n_points, int64_t mol_size, int64_t *chunk, int64_t *spm,
+                          int64_t *n_chunks) {
+    if (mol_size <= PD_DIRECT_CHUNK) {
+        *chunk = (PD_DIRECT_CHUNK / mol_size) * mol_size;
+        *spm = 1;
+        *n_chunks = (n_points + *chunk - 1) / *chunk;
+    } else {
+        *chunk = PD_DIRECT_CHUNK;
+        *spm = (mol_size + PD_DIRECT_CHUNK - 1) / PD_DIRECT_CHUNK;
+        *n_chunks = (n_points / mol_size) * *spm;
+    }
+}
+
+int64_t direct_chunks(int64_t n_points, int64_t mol_size) {
+    int64_t chunk, spm, n;
+    direct_layout(n_points, mol_size, &chunk, &spm, &n);
+    return n;
+}
+
+cudaError_t launch_direct(const double *xyz, const uint32_t *kind, const double *weight,
+                          const double *ff, const double *qvec, int64_t n_vec, int64_t n_points,
+                          int64_t mol_size, double *part, int64_t part_chunks, double *out,
+                          cudaStream_t st) {
+    int64_t chunk, spm, n_chunks;
+    direct_layout(n_points, mol_size, &chunk, &spm, &n_chunks);
+    if (n_chunks > part_chunks || n_chunks > 65535 || n_vec < 1) return cudaErrorInvalidValue;
+    const dim3 g(static_cast<unsigned>((n_vec + 127) / 128), static_cast<unsigned>(n_chunks));
+    pd_direct_chunks<<<g, 128, 0, st>>>(xyz, kind, weight, ff, qvec, n_vec, mol_size, chunk,
+                                        spm, n_points, part);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    pd_direct_reduce<<<static_cast<unsigned>((n_vec + 127) / 128), 128, 0, st>>>(
+        part, n_vec, n_chunks, spm, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_ff_eval(const int32_t *desc, const double *range, const double *params,
+                           int32_t n_ff, double qmin, double qmax, int64_t nq, int *bad,
+                           double *out, cudaStream_t st) {
+    const int64_t total = static_cast<int64_t>(n_ff) * nq;
+    pd_ff_eval<<<static_cast<unsigned>((total + 127) / 128), 128, 0, st>>>(
+        desc, range, params, n_ff, qmin, qmax, nq, bad, out);
     return cudaGetLastError();
 }
 

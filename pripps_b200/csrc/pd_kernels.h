@@ -46,7 +46,22 @@ cudaError_t launch_lattice_sums(const unsigned long long *hist, const PdLatDev *
                                 const double *qv, int32_t nq, int add_exact, const int *err,
                                 double *pairsum, cudaStream_t st);
 cudaError_t launch_frame_mean(const double *terms, const double *fw, int32_t n_frames, int32_t nq,
-                              double *out, cudaStream_t st);
+                              double *out, cudaStream_t st, bool normalize = true);
+// Direct transform: (Re A, Im A, |A|², Σ_m |F_m|²) per q-vector for points
+// in molecules of mol_size (n_points a multiple of it). part holds
+// direct_chunks(n_points, mol_size) × n_vec × 5 doubles.
+cudaError_t launch_direct(const double *xyz, const uint32_t *kind, const double *weight,
+                          const double *ff, const double *qvec, int64_t n_vec, int64_t n_points,
+                          int64_t mol_size, double *part, int64_t part_chunks, double *out,
+                          cudaStream_t st);
+int64_t direct_chunks(int64_t n_points, int64_t mol_size);
+// Form-factor tables [n_ff][nq] on the uniform grid; *bad = index + 1 of a
+// form factor whose range misses a grid point (0 if none).
+cudaError_t launch_ff_eval(const int32_t *desc, const double *range, const double *params,
+                           int32_t n_ff, double qmin, double qmax, int64_t nq, int *bad,
+                           double *out, cudaStream_t st);
+cudaError_t launch_stream_accumulate(const double *batch, double scale, int32_t n, double *acc,
+                                     cudaStream_t st);
 cudaError_t launch_ffma_probe(float *out, int iters, int grid, int block, bool packed,
                               cudaStream_t st);
 

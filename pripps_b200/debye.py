@@ -46,10 +46,14 @@ class Contributions:
 
 @dataclass
 class Intensity:
-    """I(q) on a q grid (src/lib.rs:89-109)."""
+    """I(q) on a q grid (src/lib.rs:89-109). form_factor and
+    effective_structure_factor are set by the direct transform of a box of
+    identical molecules (src/lib.rs:510-526)."""
     q: np.ndarray
     total: np.ndarray
     contributions: Optional[Contributions] = None
+    form_factor: Optional[np.ndarray] = None
+    effective_structure_factor: Optional[np.ndarray] = None
 
 
 def combine(terms: np.ndarray, volume_scale: float, contrast_density: float) -> np.ndarray:
@@ -317,7 +321,31 @@ class Pripps:
         return model.intensity(active.excluded.effective_volume_scale(),
                                active.hydration.effective_contrast_density())
 
+    def direct_intensity(self, structure, p_max: int, box_sides,
+                         solvent: Optional[SolventConfig] = None,
+                         num_molecules: Optional[int] = None, indices=None) -> Intensity:
+        """I(q) of a periodic box by the direct transform (IntensityScheme::
+        Direct, src/lib.rs:424-431 with the --num-molecules guards and
+        derivations, :365-411 and :510-526). ``indices`` replaces the Miller
+        vectors with any integer reciprocal-lattice list."""
+        from .direct import DirectTransform, check_num_molecules
+        s = self._structure(structure)
+        active = solvent if (solvent is not None and solvent.is_active()) else None
+        check_num_molecules(s, num_molecules, active is not None)
+        t = DirectTransform(self.formfactors, p_max, active, num_molecules, indices, self._ctx)
+        return t.calc_intensities(s, box_sides)
+
+    def direct_model(self, structure, p_max: int, box_sides, solvent: SolventConfig):
+        """Cached direct-transform amplitudes for fitting (src/lib.rs:305-342)."""
+        from .direct import DirectTransform
+        s = self._structure(structure)
+        t = DirectTransform(self.formfactors, p_max, solvent, None, None, self._ctx)
+        return t.build_model(s, box_sides)
+
     def _trajectory(self, s, q, qmin, qmax, active, frames, frame_weights, stride):
+        if not isinstance(frames, (np.ndarray, list, tuple)):
+            return self._trajectory_stream(s, q, qmin, qmax, active, frames, frame_weights,
+                                           stride)
         frames = np.asarray(frames, dtype=np.float64)
         if frames.ndim != 3 or frames.shape[1:] != (len(s), 3):
             raise ValidationError(
@@ -371,3 +399,81 @@ class Pripps:
             return Intensity(q, terms[0].copy(), None)
         return Intensity(q, combine(terms, active.excluded.effective_volume_scale(),
                                     active.hydration.effective_contrast_density()), None)
+
+    def _trajectory_stream(self, s, q, qmin, qmax, active, frames, frame_weights, stride,
+                           frames_per_batch: int = 64):
+        """Frames from an iterable (a reader), solved in pinned batches while
+        later frames are still being read (pd_stream_*)."""
+        if stride < 1:
+            raise ValidationError("stride must be >= 1")
+        req = make_request(s, self.formfactors, q, qmin, qmax, active, self.precision)
+        if req.lattices:
+            raise ValidationError("dummies away from the atoms depend on each frame; pass the "
+                                  "frames as an array")
+        st = TrajectoryStream(req, frames_per_batch, self.ctx)
+        buf, wts = [], []
+        for fr, w in _frame_pairs(frames, frame_weights, stride):
+            buf.append(np.asarray(fr, dtype=np.float64).reshape(len(s), 3))
+            wts.append(w)
+            if len(buf) == frames_per_batch:
+                st.push(np.stack(buf), np.array(wts))
+                buf, wts = [], []
+        if buf:
+            st.push(np.stack(buf), np.array(wts))
+        terms = st.finish()
+        if active is None:
+            return Intensity(q, terms[0].copy(), None)
+        return Intensity(q, combine(terms, active.excluded.effective_volume_scale(),
+                                    active.hydration.effective_contrast_density()), None)
+
+
+def _frame_pairs(frames, frame_weights, stride):
+    """(frame, weight) of every stride-th frame of an iterable, with the weight
+    of the original frame index (src/trajectory.rs:56-61)."""
+    wit = iter(frame_weights) if frame_weights is not None else None
+    for k, fr in enumerate(frames):
+        w = 1.0 if wit is None else float(next(wit))
+        if k % stride == 0:
+            yield fr, w
+
+
+class TrajectoryStream:
+    """A trajectory average fed frame by frame (pd_stream_*): the frame loop of
+    trajectory_average (src/trajectory.rs:198-248) for trajectories too long to
+    hold at once. ``push`` takes [F, N, 3] Å frames (and weights); pinned
+    batches of ``frames_per_batch`` frames are uploaded while the previous
+    batch is solved; ``finish`` returns the [6, nq] weighted mean of the six
+    profiles."""
+
+    def __init__(self, topology: DebyeRequest, frames_per_batch: int = 64,
+                 ctx: Optional[_lib.Context] = None):
+        self.ctx = ctx or _lib.default_context()
+        self._req = topology
+        self._nq = topology.nq
+        self._n = topology.n_atoms
+        self._h = C.c_void_p()
+        r = topology.c_struct()
+        _lib.check(_lib.lib().pd_stream_open(self.ctx.handle, C.byref(r), int(frames_per_batch),
+                                             C.byref(self._h)), self.ctx.handle)
+
+    def push(self, frames, weights=None) -> None:
+        fr = np.ascontiguousarray(frames, dtype=np.float64).reshape(-1, self._n, 3)
+        w = None if weights is None else np.ascontiguousarray(weights, dtype=np.float64)
+        if w is not None and len(w) != len(fr):
+            raise ValidationError(f"{len(w)} weights for {len(fr)} frames")
+        _lib.check(_lib.lib().pd_stream_push(self.ctx.handle, self._h, _lib.dptr(fr),
+                                             _lib.dptr(w), len(fr)), self.ctx.handle)
+
+    def finish(self) -> np.ndarray:
+        out = np.empty((6, self._nq), dtype=np.float64)
+        h, self._h = self._h, C.c_void_p()
+        _lib.check(_lib.lib().pd_stream_finish(self.ctx.handle, h, _lib.dptr(out)),
+                   self.ctx.handle)
+        return out
+
+    def __del__(self):  # pragma: no cover - an unfinished stream is released
+        try:
+            if self._h:
+                _lib.lib().pd_stream_finish(self.ctx.handle, self._h, None)
+        except Exception:
+            pass

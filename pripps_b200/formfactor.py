@@ -218,10 +218,16 @@ class FormFactorMap:
                 return e.formfactor
         return None
 
-    def table(self, ids: Sequence[int], q_values: np.ndarray) -> np.ndarray:
+    def table(self, ids: Sequence[int], q_values: np.ndarray, ctx=None,
+              grid: Optional[Tuple[float, float, int]] = None) -> np.ndarray:
         """[len(ids) × nq] FP64 table of F_id(q_k). Only the listed ids are
         evaluated, so unused species with narrower q ranges never raise
-        (src/formfactor.rs:520-544)."""
+        (src/formfactor.rs:520-544). With a device context and the uniform
+        grid (qmin, qmax, nq) that q_values holds, the table is evaluated on
+        the device (pd_formfactor_tables)."""
+        if ctx is not None and grid is not None:
+            return device_tables([self.entries[i].formfactor for i in ids], grid[0], grid[1],
+                                 grid[2], ctx)
         out = np.empty((len(ids), len(q_values)), dtype=np.float64)
         for r, idx in enumerate(ids):
             ff = self.entries[idx].formfactor
@@ -392,3 +398,51 @@ def read_formfactors(path) -> FormFactorMap:
     """Read a form-factor YAML file (src/formfactor.rs:446-454)."""
     with open(path, "r", encoding="utf-8") as fh:
         return formfactors_from_yaml_str(fh.read())
+
+
+# ------------------------------------------------------ device evaluation
+# Kind codes of pd_formfactor (include/pripps_debye.h).
+PD_FF_CODES = {"Constant": 0, "Gaussian": 1, "SingleGaussian": 2, "Polynomial": 3, "Table": 4}
+
+
+def device_descriptor(ff: FormFactor):
+    """(type, n, qlo, qhi, params) of a runtime form factor for
+    pd_formfactor_tables."""
+    lo, hi = ff.qrange()
+    if isinstance(ff, Constant):
+        return 0, 1, lo, hi, [float(ff.c)]
+    if isinstance(ff, Gaussian):
+        return 1, len(ff.ab), lo, hi, [float(ff.c)] + [float(x) for ab in ff.ab for x in ab]
+    if isinstance(ff, SingleGaussian):
+        return 2, 1, lo, hi, [float(ff.a), float(ff.b)]
+    if isinstance(ff, Polynomial):
+        return 3, len(ff.coeff), lo, hi, [float(c) for c in ff.coeff]
+    if isinstance(ff, Table):
+        return 4, len(ff._xs), lo, hi, [float(x) for x in ff._xs] + [float(y) for y in ff._ys]
+    raise ValidationError(f"form factor {type(ff).__name__} has no device form")
+
+
+def device_tables(ffs: Sequence[FormFactor], qmin: float, qmax: float, nq: int, ctx) -> np.ndarray:
+    """[len(ffs) × nq] F(q_k) on the uniform grid, evaluated on the device
+    (pd_formfactor_tables); a grid point outside a form factor's range raises
+    QOutOfRange, as FormFactor::eval does (src/formfactor.rs:188-193)."""
+    import ctypes as C
+    from . import _lib
+    descs = (_lib.PdFormFactor * len(ffs))()
+    keep = []
+    for k, ff in enumerate(ffs):
+        t, n, lo, hi, par = device_descriptor(ff)
+        arr = np.ascontiguousarray(par, dtype=np.float64)
+        keep.append(arr)
+        descs[k].type, descs[k].n, descs[k].qlo, descs[k].qhi = t, n, lo, hi
+        descs[k].params = _lib.dptr(arr)
+    out = np.empty((len(ffs), int(nq)), dtype=np.float64)
+    rc = _lib.lib().pd_formfactor_tables(ctx.handle, descs, len(ffs), float(qmin), float(qmax),
+                                         int(nq), _lib.dptr(out))
+    if rc == _lib.PD_EINVAL and "QOutOfRange" in _lib.last_error(ctx.handle):
+        q = linear_q_values(qmin, qmax, nq)
+        for ff in ffs:  # name the first failing point as the host evaluator would
+            for x in q:
+                ff.eval(float(x))
+    _lib.check(rc, ctx.handle)
+    return out

@@ -178,6 +178,40 @@ def stream_request(sr: synth.StreamRequest, precision="fp32") -> Workload:
                     globule_request(g, 0.0, sr.qmax, sr.nq, sr.solvent, precision), g)
 
 
+class GlobulePool:
+    """Compact sub-globules for long request streams: a few RSA globules at
+    log-spaced sizes, atoms sorted by distance from the centre; a request of N
+    atoms takes the N innermost atoms of the smallest pool globule that has
+    them (the same packing density as a globule built for N, without an RSA
+    run per request), with surface exposure redrawn for its own envelope."""
+
+    def __init__(self, n_min: int = 500, n_max: int = 50_000, size: int = 24, seed: int = 40):
+        self.globules = []
+        for k, n in enumerate(np.unique(np.geomspace(n_min, n_max, size).astype(np.int64))):
+            r = synth.sphere_radius_for(int(n))
+            g = synth.globule(int(n), (r, r, r), seed + k)
+            c = g.pos.mean(axis=0)
+            order = np.argsort(np.linalg.norm(g.pos - c, axis=1), kind="stable")
+            self.globules.append((int(n), g.pos[order] - c, g.elements[order]))
+
+    def take(self, n: int, seed: int) -> synth.Globule:
+        for size, pos, el in self.globules:
+            if size >= n:
+                break
+        p, e = pos[:n], el[:n]
+        rad = np.linalg.norm(p, axis=1)
+        rng = np.random.default_rng(seed)
+        exposed = (rad >= rad.max() - 3.0) & (rng.random(n) < synth.EXPOSED_PROB)
+        return synth.Globule(p.copy(), e.copy(), exposed, (rad.max(),) * 3)
+
+
+def stream_request_pooled(sr: synth.StreamRequest, pool: GlobulePool,
+                          precision="fp32") -> Workload:
+    g = pool.take(sr.n_atoms, sr.seed)
+    return Workload(f"stream_{sr.n_atoms}",
+                    globule_request(g, 0.0, sr.qmax, sr.nq, sr.solvent, precision), g)
+
+
 def small_globule(n: int, seed: int, nq: int = 40, qmax: float = 0.5, solvent: bool = True,
                   precision: str = "fp32", radius: Optional[float] = None) -> Workload:
     r = radius if radius is not None else synth.sphere_radius_for(max(n, 8))
