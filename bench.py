@@ -206,9 +206,14 @@ def run_ours(args, ws, rank, local):
     ctx = _lib.Context(local)
     lib = _lib.lib()
 
-    peak_ffma, peak_ffma2 = C.c_double(), C.c_double()
-    _lib.check(lib.pd_measure_fp32_peak(ctx.handle, C.byref(peak_ffma), C.byref(peak_ffma2)),
-               ctx.handle)
+    # FP32 issue peak: best of three probe runs (a single short probe reads a
+    # few % low when the power state is still settling)
+    peak_ffma, peak_ffma2 = C.c_double(0.0), C.c_double(0.0)
+    for _ in range(3):
+        a, b = C.c_double(), C.c_double()
+        _lib.check(lib.pd_measure_fp32_peak(ctx.handle, C.byref(a), C.byref(b)), ctx.handle)
+        peak_ffma.value = max(peak_ffma.value, a.value)
+        peak_ffma2.value = max(peak_ffma2.value, b.value)
 
     # ---- device-resident path
     r = req.c_struct()
@@ -353,7 +358,8 @@ def run_ours(args, ws, rank, local):
                          "kernel": "pd_pairs_fp32", "flops_per_pair_q": flops,
                          "kernel_pair_q_per_launch": kernel_pair_q,
                          "kernel_ms_per_launch": launch_ms,
-                         "peak_source": "measured FFMA probe (pd_measure_fp32_peak), this run",
+                         "peak_source": "measured FFMA probe (pd_measure_fp32_peak), best of "
+                                        "3 in this run",
                          "peak_ffma2_tflops": peak_ffma2.value,
                          "theoretical_peak_tflops_at_max_clock":
                              2 * 128 * 148 * (clk["sm_max_mhz"] or 1965.0) * 1e-6},

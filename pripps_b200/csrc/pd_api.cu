@@ -233,7 +233,7 @@ struct DevPlan {
     }
 };
 
-Tuning tuning_for(pd_ctx *ctx, int64_t n, int64_t nq, int precision) {
+Tuning tuning_for(pd_ctx *ctx, int64_t n, int64_t nq, int precision, int64_t n_frames = 1) {
     const int nb = static_cast<int>(std::floor(std::log2(static_cast<double>(std::max<int64_t>(n, 1)))));
     const int qb = static_cast<int>(std::floor(std::log2(static_cast<double>(std::max<int64_t>(nq, 1)))));
     if (ctx) {
@@ -245,7 +245,7 @@ Tuning tuning_for(pd_ctx *ctx, int64_t n, int64_t nq, int precision) {
             return t;
         }
     }
-    return pd::default_tuning(n, nq, precision);
+    return pd::default_tuning(n, nq, precision, n_frames);
 }
 
 void free_devplan(pd_ctx *ctx, DevPlan &dp, cudaStream_t st) {
@@ -327,7 +327,8 @@ int plan_host(pd_ctx *ctx, const pd_request *req, const uint32_t *species, const
               bool host_xyz, DevPlan &dp) {
     std::string msg;
     Tuning tun = tuning_for(ctx, static_cast<int64_t>(req->n_atoms),
-                            static_cast<int64_t>(req->nq), static_cast<int>(req->precision));
+                            static_cast<int64_t>(req->nq), static_cast<int>(req->precision),
+                            static_cast<int64_t>(req->n_frames));
     int rc = pd::build_plan(req, species, weights, tun, dp.P, msg);
     if (rc != PD_OK) {
         ctx->set_error(msg);
@@ -1220,7 +1221,8 @@ int pd_plan_tiles(pd_ctx *ctx, const pd_request *req, uint32_t rank, uint32_t wo
         return rc;
     }
     Tuning tun = tuning_for(ctx, static_cast<int64_t>(req->n_atoms), static_cast<int64_t>(req->nq),
-                            static_cast<int>(req->precision));
+                            static_cast<int>(req->precision),
+                            static_cast<int64_t>(req->n_frames));
     Plan P;
     rc = pd::build_plan(req, req->species, req->hyd_weights, tun, P, msg);
     if (rc) {
@@ -1493,7 +1495,8 @@ int pd_plan_inspect(pd_ctx *ctx, const pd_request *req, uint64_t *n_classes, uin
         return rc;
     }
     Tuning tun = tuning_for(ctx, static_cast<int64_t>(req->n_atoms), static_cast<int64_t>(req->nq),
-                            static_cast<int>(req->precision));
+                            static_cast<int>(req->precision),
+                            static_cast<int64_t>(req->n_frames));
     Plan P;
     rc = pd::build_plan(req, req->species, req->hyd_weights, tun, P, msg, /*count_pairs=*/true);
     if (rc) {
@@ -2066,7 +2069,8 @@ extern "C" int pd_solve_noalloc(const pd_request *req, const double *xyz_dev,
     if (rc) return noalloc_fail(rc, "pd_solve_noalloc: " + msg);
     DevPlan dp;
     Tuning tun = tuning_for(nullptr, static_cast<int64_t>(r.n_atoms), static_cast<int64_t>(r.nq),
-                            static_cast<int>(r.precision));
+                            static_cast<int>(r.precision),
+                            static_cast<int64_t>(r.n_frames));
     rc = pd::build_plan(&r, r.species, r.hyd_weights, tun, dp.P, msg);
     if (rc) return noalloc_fail(rc, "pd_solve_noalloc: " + msg);
     dp.L = make_layout(dp.P, false);

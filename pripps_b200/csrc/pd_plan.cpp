@@ -178,7 +178,7 @@ static int next_pow2(int64_t v) {
     return p;
 }
 
-Tuning default_tuning(int64_t n_atoms, int64_t nq, int precision) {
+Tuning default_tuning(int64_t n_atoms, int64_t nq, int precision, int64_t n_frames) {
     Tuning t;
     if (precision == PD_FP64) {
         t.K = 32;
@@ -205,7 +205,21 @@ Tuning default_tuning(int64_t n_atoms, int64_t nq, int precision) {
         t.K = 32;
         t.NP = 4;
     }
+    // j chunk: about N/8 atoms, halved while a solve would have fewer than
+    // ~6 tiles per resident CTA of a B200 (148 SMs × 3): the longest-first
+    // tile order then ends with short tiles on every SM. Measured step times
+    // (pair kernel + slot reduction): 10,000 atoms, nq 500: 3.82 / 3.51 /
+    // 3.54 / 3.74 ms at 2,048 / 1,024 / 512 / 256; 20,000 atoms, nq 512:
+    // 13.24 / 12.78 / 12.89 ms at 4,096 / 2,048 / 1,024; 100,000 atoms, nq
+    // 1,000: 589.5 / 592.5 ms at 16,384 / 4,096.
     t.TJ = std::clamp(next_pow2(n_atoms / 8), 256, 16384);
+    const double iblocks = static_cast<double>((n_atoms + 127) / 128);
+    const double nqb = static_cast<double>((nq + t.K - 1) / t.K);
+    const double frames = static_cast<double>(std::max<int64_t>(n_frames, 1));
+    while (t.TJ > 256 &&
+           iblocks * std::ceil(static_cast<double>(n_atoms) / t.TJ) * 0.5 * nqb * frames <
+               6.0 * 148 * 3)
+        t.TJ /= 2;
     return t;
 }
 

@@ -74,7 +74,7 @@ struct Plan {
 int validate_request(const pd_request *req, bool device_pointers, std::string &msg);
 
 // Default shape when no tuned entry exists.
-Tuning default_tuning(int64_t n_atoms, int64_t nq, int precision);
+Tuning default_tuning(int64_t n_atoms, int64_t nq, int precision, int64_t n_frames = 1);
 
 // Build the plan from host-side species and weights (hyd may be NULL).
 // count_pairs fills Plan::pairs_covered (an O(N · tiles per block) host loop
