@@ -447,6 +447,57 @@ def run_serve(args, ws, rank, local):
     ctx.close()
 
 
+def run_direct(args, ws, rank, local):
+    """Direct transform of a periodic box (pd_direct): 64 copies of a
+    2,000-atom globule on a 4×4×4 grid in a 320 Å box, Miller vectors with
+    p_max = args.p_max, per-molecule self terms. Unit: (q-vector, point)
+    amplitude terms per second; the oracle's rows on a sample beside it."""
+    import torch
+    from oracle import oracle as O
+    from pripps_b200 import _lib, synth, workloads
+    from pripps_b200.direct import amplitudes, miller_indices, q_vectors
+    torch.cuda.set_device(local)
+    ctx = _lib.Context(local)
+    g = synth.globule(2000, (25.0, 25.0, 25.0), 9)
+    L = 320.0
+    offs = [(i, j, k) for i in range(4) for j in range(4) for k in range(4)]
+    xyz = np.concatenate([g.pos + 80.0 * np.array(o) + 40.0 for o in offs])
+    ids = workloads.element_ids()[np.tile(g.elements, len(offs))]
+    used = np.unique(ids)
+    kind = np.searchsorted(used, ids)
+    qv = q_vectors(miller_indices(args.p_max), [L] * 3)
+    qn = np.sqrt((qv * qv).sum(axis=1))
+    ff = workloads.foxs().table(used, qn)
+    for _ in range(args.warmup):
+        amplitudes(xyz, kind, ff, qv, len(offs), None, ctx)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        rows = amplitudes(xyz, kind, ff, qv, len(offs), None, ctx)
+        times.append(time.perf_counter() - t0)
+    work = len(qv) * len(xyz)
+    ms = 1e3 * sum(times) / len(times)
+    # oracle on a sample: the first 8 molecules (16,000 points), 39 vectors
+    nsamp = 16000
+    t0 = time.perf_counter()
+    O.direct_rows(xyz[:nsamp], kind[:nsamp], ff[:, :39], qv[:39], 8)
+    dt = time.perf_counter() - t0
+    if rank == 0:
+        print(json.dumps({
+            "metric": "Direct transform (q-vector, point) terms/s", "value": work / (ms * 1e-3),
+            "unit": "vector·point/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "direct_box_64x2000", "points": len(xyz), "molecules": 64,
+                       "box": L, "p_max": args.p_max, "vectors": len(qv),
+                       "timed": "blocking pd_direct with host buffers (upload, kernels, download)"},
+            "cpu_baseline": {"value": nsamp * 39 / dt, "unit": "vector·point/s", "cores": 1,
+                             "kind": "port", "sample": "16,000 points x 39 vectors",
+                             "seconds": dt},
+            "checksum_selfterm": float(rows[:, 3].sum())}), flush=True)
+    ctx.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -462,6 +513,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--serve", action="store_true", help="serving-stream benchmark")
+    ap.add_argument("--direct", action="store_true", help="direct-transform benchmark")
+    ap.add_argument("--p-max", type=int, default=100)
     ap.add_argument("--requests", type=int, default=200)
     ap.add_argument("--rate", type=float, default=20.0, help="Poisson arrival rate (1/s)")
     ap.add_argument("--budget-gb", type=float, default=40.0)
@@ -472,6 +525,8 @@ def main():
         run_reference(args, ws, rank)
     elif args.serve:
         run_serve(args, ws, rank, local)
+    elif args.direct:
+        run_direct(args, ws, rank, local)
     else:
         run_ours(args, ws, rank, local)
 

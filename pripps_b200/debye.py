@@ -323,7 +323,8 @@ class Pripps:
 
     def direct_intensity(self, structure, p_max: int, box_sides,
                          solvent: Optional[SolventConfig] = None,
-                         num_molecules: Optional[int] = None, indices=None) -> Intensity:
+                         num_molecules: Optional[int] = None, indices=None,
+                         grid=None) -> Intensity:
         """I(q) of a periodic box by the direct transform (IntensityScheme::
         Direct, src/lib.rs:424-431 with the --num-molecules guards and
         derivations, :365-411 and :510-526). ``indices`` replaces the Miller
@@ -332,7 +333,8 @@ class Pripps:
         s = self._structure(structure)
         active = solvent if (solvent is not None and solvent.is_active()) else None
         check_num_molecules(s, num_molecules, active is not None)
-        t = DirectTransform(self.formfactors, p_max, active, num_molecules, indices, self._ctx)
+        t = DirectTransform(self.formfactors, p_max, active, num_molecules, indices, self._ctx,
+                            grid)
         return t.calc_intensities(s, box_sides)
 
     def direct_model(self, structure, p_max: int, box_sides, solvent: SolventConfig):

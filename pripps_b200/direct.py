@@ -15,8 +15,10 @@ and hydration dummies each get their amplitudes, cached in a DirectModel
 that recombines |A − v·C + c·B|² per vector before grouping
 (src/explicit.rs:296-357).
 
-The reference's lattice q-grid builder (QGrid::lattice, src/q_grid.rs) is not
-restated: a caller with such a grid passes its integer indices directly.
+The q grids (src/q_grid.rs) are restated in QGrid: the Miller grid, and the
+lattice grid of every reciprocal-lattice vector up to q_max in |q| bins
+(exact shells, evenly spread subsets of large bins, spherical-Fibonacci
+sampling of bins beyond ~20,000 vectors).
 """
 from __future__ import annotations
 
@@ -140,10 +142,15 @@ class DirectTransform:
 
     def __init__(self, formfactors: FormFactorMap, p_max: int = 6,
                  solvent: Optional[SolventConfig] = None, num_molecules: Optional[int] = None,
-                 indices: Optional[np.ndarray] = None, ctx: Optional[_lib.Context] = None):
+                 indices: Optional[np.ndarray] = None, ctx: Optional[_lib.Context] = None,
+                 grid: Optional["QGrid"] = None):
         self.formfactors = formfactors
-        self.indices = (miller_indices(p_max) if indices is None
-                        else np.asarray(indices, dtype=np.int64).reshape(-1, 3))
+        self.grid = grid
+        if grid is not None:
+            self.indices = grid.indices()
+        else:
+            self.indices = (miller_indices(p_max) if indices is None
+                            else np.asarray(indices, dtype=np.int64).reshape(-1, 3))
         self.solvent = solvent if (solvent is not None and solvent.is_active()) else None
         self.num_molecules = num_molecules
         self._ctx = ctx
@@ -155,6 +162,8 @@ class DirectTransform:
     def calc_intensities(self, structure: Structure, box_sides) -> Intensity:
         if box_sides is None:
             raise UsageError("direct Fourier transform requires box side lengths on the structure")
+        if self.grid is not None:
+            self.grid.check_box(box_sides)
         qvec = q_vectors(self.indices, box_sides)
         qnorm = np.sqrt(np.sum(qvec * qvec, axis=1))
         if self.solvent is not None:
@@ -166,7 +175,10 @@ class DirectTransform:
         ff = _kind_table(used, self.formfactors, qnorm)
         n = self.num_molecules or 1
         rows = amplitudes(structure.pos, kind, ff, qvec, n, ctx=self.ctx)
-        q, g = average_by_qnorm(qnorm, rows[:, 2:4])
+        if self.grid is not None:
+            q, g = self.grid.group(qnorm, rows[:, 2:4])
+        else:
+            q, g = average_by_qnorm(qnorm, rows[:, 2:4])
         out = Intensity(q, g[:, 0].copy())
         if self.num_molecules:
             self_term = g[:, 1]
@@ -233,3 +245,215 @@ def check_num_molecules(structure: Structure, n: Optional[int], solvent_active: 
         raise ValidationError(f"--num-molecules {n} does not partition the box into {n} "
                               "identical contiguous molecules: the atom composition differs "
                               "between blocks")
+
+
+# ------------------------------------------------------------------ q grids
+EXACT_BIN_LIMIT = 20_000.0               # src/q_grid.rs:170-173
+GOLDEN_ANGLE = 2.399_963_229_728_653     # src/q_grid.rs:306
+
+
+def _round(x: float) -> int:
+    """f64::round: halves away from zero."""
+    return int(math.floor(x + 0.5)) if x >= 0 else -int(math.floor(-x + 0.5))
+
+
+def _bin_width(box) -> float:
+    return 2.0 * math.pi / max(0.0, *box)
+
+
+def _expected_count(box, k: int) -> float:
+    """src/q_grid.rs:179-184"""
+    width = _bin_width(box)
+    volume = box[0] * box[1] * box[2]
+    return 2.0 * math.pi * (k * width) ** 2 * width * volume / (2.0 * math.pi) ** 3
+
+
+def _largest_exact_bin(box) -> int:
+    k = 1
+    while not _expected_count(box, k + 1) > EXACT_BIN_LIMIT:
+        k += 1
+    return k
+
+
+def _upper_half(n) -> bool:
+    h, k, l = n
+    return h > 0 or (h == 0 and (k > 0 or (k == 0 and l > 0)))
+
+
+def _norm(box, n) -> float:
+    s = 0.0
+    for a in range(3):
+        s += (2.0 * math.pi * n[a] / box[a]) ** 2
+    return math.sqrt(s)
+
+
+def _exact_shells(box, q_max: float):
+    """src/q_grid.rs:315-344: every upper-half lattice vector with
+    |q| <= q_max in the exactly enumerated bins, grouped by bin."""
+    width = _bin_width(box)
+    last_exact = _largest_exact_bin(box)
+    q_max = min(q_max, (last_exact + 0.5) * width)
+    n_max = [int(math.floor(q_max * (1.0 + 1e-12) * l / (2.0 * math.pi))) for l in box]
+    bins = {}
+    for h in range(-n_max[0], n_max[0] + 1):
+        for k in range(-n_max[1], n_max[1] + 1):
+            for l in range(-n_max[2], n_max[2] + 1):
+                n = (h, k, l)
+                if not _upper_half(n):
+                    continue
+                q = _norm(box, n)
+                b = _round(q / width)
+                if q <= q_max * (1.0 + 1e-12) and b <= last_exact:
+                    bins.setdefault(b, []).append((n, q))
+    return [bins[b] for b in sorted(bins)]
+
+
+def _direction_key(n) -> float:
+    x, y, z = (float(c) for c in n)
+    norm = math.sqrt(x * x + y * y + z * z)
+    band = math.floor((z / norm + 1.0) * 8.0)
+    return band * 10.0 + math.atan2(y, x)
+
+
+def _spread_subset(shell, cap: int):
+    """src/q_grid.rs:351-359"""
+    if len(shell) <= cap:
+        return list(shell)
+    shell.sort(key=lambda v: _direction_key(v[0]))
+    return [shell[i * len(shell) // cap] for i in range(cap)]
+
+
+def _shell_holds(box, a, b, n) -> bool:
+    length = _norm(box, n)
+    return a <= length < b
+
+
+def _shell_any_vector(box, a, b):
+    """src/q_grid.rs:279-303"""
+    step = [2.0 * math.pi / l for l in box]
+    n_max = [int(math.floor(b / s)) for s in step]
+    for h in range(0, n_max[0] + 1):
+        for k in range(-n_max[1], n_max[1] + 1):
+            planar = (h * step[0]) ** 2 + (k * step[1]) ** 2
+            if planar >= b * b:
+                continue
+            l0 = int(math.ceil(math.sqrt(max(a * a - planar, 0.0)) / step[2]))
+            for l in (l0 - 1, l0, l0 + 1):
+                n = (h, k, l) if _upper_half((h, k, l)) else (-h, -k, -l)
+                if _upper_half(n) and _shell_holds(box, a, b, n):
+                    return n
+    return None
+
+
+def _sampled_shell(box, k: int, q_max: float, cap: int):
+    """src/q_grid.rs:194-262: spherical-Fibonacci directions at radii uniform
+    in the shell volume, snapped to the lattice and deduplicated."""
+    width = _bin_width(box)
+    a, b = (k - 0.5) * width, min((k + 0.5) * width, q_max)
+    if b <= a:
+        return None
+    q = 0.75 * (b ** 4 - a ** 4) / (b ** 3 - a ** 3)
+    sb = min((k + 0.5) * width, q_max * (1.0 + 1e-12))
+    wanted = min(cap, int(EXACT_BIN_LIMIT))
+    attempts = 2 * wanted + 16
+    seen, vectors = set(), []
+    for i in range(attempts):
+        z = 1.0 - (2 * i + 1) / attempts
+        sn, cs = math.sin(i * GOLDEN_ANGLE), math.cos(i * GOLDEN_ANGLE)
+        rho = math.sqrt(1.0 - z * z)
+        tt = i * 0.618_033_988_749_895
+        t = tt - math.trunc(tt)
+        r = math.cbrt(a ** 3 + t * (b ** 3 - a ** 3))
+        direction = (rho * cs, rho * sn, z)
+        n = tuple(_round(r * direction[ax] * box[ax] / (2.0 * math.pi)) for ax in range(3))
+        if not _upper_half(n):
+            n = tuple(-c for c in n)
+        if _upper_half(n) and _shell_holds(box, a, sb, n) and n not in seen:
+            seen.add(n)
+            vectors.append(n)
+    if not vectors:
+        v = _shell_any_vector(box, a, sb)
+        return None if v is None else (q, [v])
+    m = min(wanted, len(vectors))
+    return q, [vectors[i * len(vectors) // m] for i in range(m)]
+
+
+class QGrid:
+    """Which q-vectors a periodic box is sampled at (src/q_grid.rs): the 13
+    Miller directions × p, or every reciprocal-lattice vector up to q_max in
+    |q| bins of width 2π/max(L) (exact bins up to ~20,000 vectors, sampled
+    beyond; bins over `max_per_bin` keep an evenly spread subset)."""
+
+    def __init__(self, p_max: Optional[int] = None, box=None, vectors=None, bins=None, q=None):
+        self.p_max, self.box = p_max, box
+        self._vectors, self._bins, self._q = vectors, bins, q
+
+    @classmethod
+    def miller(cls, p_max: int) -> "QGrid":
+        return cls(p_max=int(p_max))
+
+    @classmethod
+    def lattice(cls, box_sides, q_max: float, max_per_bin: int) -> "QGrid":
+        box = [float(l) for l in box_sides]
+        if not all(math.isfinite(l) and l > 0.0 for l in box):
+            raise UsageError(f"invalid box sides {box}")
+        if not (math.isfinite(q_max) and q_max > 0.0):
+            raise UsageError(f"invalid q_max {q_max} Å⁻¹")
+        shells = _exact_shells(box, float(q_max))
+        if not shells:
+            raise UsageError(f"q_max {q_max} Å⁻¹ is below the shortest lattice vector of box "
+                             f"{box}")
+        cap = max(int(max_per_bin), 1)
+        vectors, bins, qs = [], [], []
+        for shell in shells:
+            q = sum(v[1] for v in shell) / len(shell)
+            b = len(qs)
+            qs.append(q)
+            for n, _ in _spread_subset(shell, cap):
+                vectors.append(n)
+                bins.append(b)
+        width = _bin_width(box)
+        first_sampled = _largest_exact_bin(box) + 1
+        last = _round(q_max / width)
+        for k in range(first_sampled, last + 1):
+            got = _sampled_shell(box, k, float(q_max), cap)
+            if got is not None:
+                b = len(qs)
+                qs.append(got[0])
+                for n in got[1]:
+                    vectors.append(n)
+                    bins.append(b)
+        return cls(box=box, vectors=np.array(vectors, dtype=np.int64).reshape(-1, 3),
+                   bins=np.array(bins, dtype=np.int64), q=np.array(qs))
+
+    @property
+    def is_lattice(self) -> bool:
+        return self._vectors is not None
+
+    def indices(self) -> np.ndarray:
+        return self._vectors if self.is_lattice else miller_indices(self.p_max)
+
+    def q(self) -> np.ndarray:
+        return self._q if self.is_lattice else np.zeros(0)
+
+    def vectors_per_bin(self):
+        if not self.is_lattice:
+            return []
+        return np.bincount(self._bins, minlength=len(self._q)).tolist()
+
+    def check_box(self, box_sides) -> None:
+        if not self.is_lattice:
+            return
+        if not all(abs(box_sides[a] - self.box[a]) <= 1e-9 * self.box[a] for a in range(3)):
+            raise UsageError(f"box {list(box_sides)} differs from the {self.box} the q-grid was "
+                             "built for")
+
+    def group(self, qnorm: np.ndarray, values: np.ndarray):
+        """Mean of the rows per |q| group (src/q_grid.rs:140-157)."""
+        if not self.is_lattice:
+            return average_by_qnorm(qnorm, values)
+        sums = np.zeros((len(self._q), values.shape[1]))
+        for r, b in enumerate(self._bins):
+            sums[b] = sums[b] + values[r]
+        counts = np.array(self.vectors_per_bin(), dtype=np.float64)
+        return self._q.copy(), sums / counts[:, None]

@@ -87,3 +87,24 @@ def test_direct_model_with_solvent_matches_oracle_amplitudes(gpu_ctx):
     scale = np.abs(a).max() ** 2
     assert np.max(np.abs(got.total - ref[:, 0]) / scale) < 1e-12
     assert np.max(np.abs(got.contributions.atoms - ref[:, 1]) / scale) < 1e-12
+
+
+def test_lattice_grid_direct_intensity_matches_oracle(gpu_ctx):
+    """A lattice q-grid (QGrid.lattice): per-vector |A|² from the device,
+    averaged per bin as the reference's QGrid::group (src/q_grid.rs:140-157)."""
+    from pripps_b200 import Pripps, Structure
+    from pripps_b200.direct import QGrid
+    g = workloads.small_globule(300, 3).globule
+    ids = workloads.element_ids()[g.elements]
+    L = 120.0
+    s = Structure(g.pos + L / 2, ids)
+    m = workloads.foxs()
+    grid = QGrid.lattice([L] * 3, 0.35, 40)
+    got = Pripps(m, ctx=gpu_ctx).direct_intensity(s, 0, [L] * 3, grid=grid)
+    qv = q_vectors(grid.indices(), [L] * 3)
+    qn = np.sqrt((qv * qv).sum(axis=1))
+    used = np.unique(ids)
+    rows = O.direct_rows(s.pos, np.searchsorted(used, ids), m.table(used, qn), qv)
+    q, ref = grid.group(qn, rows[:, 2:3])
+    assert np.array_equal(got.q, q)
+    assert np.max(np.abs(got.total - ref[:, 0]) / np.abs(ref[:, 0]).max()) < 1e-12
