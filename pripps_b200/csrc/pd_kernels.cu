@@ -340,7 +340,8 @@ __device__ __forceinline__ void pairs_range_x2(const float4 *__restrict__ at, in
                                                int i, bool ivalid, int j0, int j1, float qs_hi,
                                                float qs_lo, float dq_hi, float dq_lo,
                                                const float2 *__restrict__ s_qres2,
-                                               float2 (&acc)[K / 2], int nchunk) {
+                                               float2 (&acc)[K / 2], int nchunk,
+                                               int rchunk = K / 16) {
     static_assert(K % 16 == 0, "K must be a multiple of 16");
     if (j0 >= j1) return;
     SeedGroup<PD_MODE_CLASS, NP, RESID, GENERAL_STEP> cur;
@@ -363,7 +364,9 @@ __device__ __forceinline__ void pairs_range_x2(const float4 *__restrict__ at, in
 #pragma unroll
         for (int t = 0; t < K / 2; ++t) {
             if ((t % 8) == 0 && t / 8 >= nchunk) break;
-            if (RESID) acc[t] = __ffma2_rn(mvs, s_qres2[t + qoff], acc[t]);
+            // the residual points are a prefix of the block: only its first
+            // rchunk 16-point chunks subtract q
+            if (RESID && (t / 8) < rchunk) acc[t] = __ffma2_rn(mvs, s_qres2[t + qoff], acc[t]);
             // d-steps of all pairs, then the accumulations, then the
             // v-steps: every instruction's operands are a group old
             // (measured 0.5 % faster than the per-pair order).
@@ -440,13 +443,20 @@ __global__ void __launch_bounds__(PD_THREADS, fp32_min_blocks(K, MODE, NP))
         const int kq0 = jb.qb * K;
         const double radius = rq.radius[jb.frame];
         const bool resid = kq0 < rq.nq && residual_q(rq.qv[kq0], radius);
+        int nres = 0;  // leading grid points of the block in the residual form
         if (resid) {
-            for (int t = threadIdx.x; t < K; t += PD_THREADS) {
-                const int kq = kq0 + t;
-                const bool on = kq < rq.nq && residual_q(rq.qv[kq], radius);
-                s_qres[t] = on ? static_cast<float>(rq.qv[kq]) : 0.0f;
+            for (int base = 0; base < K; base += PD_THREADS) {
+                const int t = base + threadIdx.x;
+                bool on = false;
+                if (t < K) {
+                    const int kq = kq0 + t;
+                    on = kq < rq.nq && residual_q(rq.qv[kq], radius);
+                    s_qres[t] = on ? static_cast<float>(rq.qv[kq]) : 0.0f;
+                }
+                nres += __syncthreads_count(on);
             }
         }
+        const int rchunk = (nres + 15) >> 4;
         __syncthreads();  // s_qres ready; every thread has read s_job
         const float4 *__restrict__ at = rq.atoms32 + static_cast<size_t>(jb.frame) * rq.n_pad;
         const int i = jb.i0 + threadIdx.x;
@@ -492,10 +502,12 @@ __global__ void __launch_bounds__(PD_THREADS, fp32_min_blocks(K, MODE, NP))
                 if (resid) {
                     if (general_step)
                         pairs_range_x2<K, NP, true, true>(chunk, jss, pi, i, ivalid, js, je, qs_hi,
-                                                          qs_lo, dq_hi, dq_lo, q2, acc, K / 16);
+                                                          qs_lo, dq_hi, dq_lo, q2, acc, K / 16,
+                                                          rchunk);
                     else
                         pairs_range_x2<K, NP, true, false>(chunk, jss, pi, i, ivalid, js, je, qs_hi,
-                                                           qs_lo, dq_hi, dq_lo, q2, acc, K / 16);
+                                                           qs_lo, dq_hi, dq_lo, q2, acc, K / 16,
+                                                           rchunk);
                 } else {
                     if (general_step)
                         pairs_range_x2<K, NP, false, true>(chunk, jss, pi, i, ivalid, js, je, qs_hi,
