@@ -1,8 +1,8 @@
 /*
  * FP64 CPU oracle for the pripps Debye path.
  *
- * TEST INFRASTRUCTURE ONLY. This file is the checker the parity tests and the
- * CPU-baseline leg of bench.py compare against; no product code path links,
+ * TEST INFRASTRUCTURE ONLY. The parity tests and the CPU-baseline leg of
+ * bench.py compare the backend against this file; no product code path links,
  * loads or calls it. It restates, loop for loop, the reference's f64 Debye
  * code so that results can be compared on identical inputs:
  *
@@ -128,7 +128,7 @@ double pdo_combine(const double *t6, double volume_scale, double contrast_densit
            2.0 * contrast_density * t6[4] - 2.0 * volume_scale * contrast_density * t6[5];
 }
 
-/* ---- q-parallel driver (rayon par_iter stand-in) ---- */
+/* ---- q-parallel loop (rayon par_iter stand-in) ---- */
 
 typedef struct {
     size_t n;

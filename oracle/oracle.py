@@ -1,8 +1,8 @@
 """ctypes front end of the FP64 CPU oracle (debye_oracle.c).
 
 TEST INFRASTRUCTURE ONLY: the parity tests, ``__graft_entry__.smoke()`` and
-the CPU-baseline legs of bench.py use it as the checker. The product path
-(pripps_b200) never imports it.
+the CPU-baseline legs of bench.py compare the backend against it. The product
+path (pripps_b200) never imports it.
 
 Every function restates the reference's f64 Debye code on the same inputs the
 CUDA backend receives (see debye_oracle.c for the file:line map).
