@@ -360,3 +360,32 @@ def test_autotune_and_fp32_probe(gpu_ctx):
     a, b = C.c_double(), C.c_double()
     assert lib.pd_measure_fp32_peak(gpu_ctx.handle, C.byref(a), C.byref(b)) == 0
     assert 10.0 < a.value < 200.0
+
+
+def test_serving_more_kernel_variants_than_lanes(gpu_ctx):
+    """Requests of six kernel variants in flight together (FP32 class K = 128
+    and K = 64, FP32 weighted, FP64 class, FP64 weighted, grid solvent with
+    lattice sets): a step runs at most four variants, the others wait for the
+    next step; every result still equals its solo solve bit for bit."""
+    from pripps_b200.serving import Server
+    rng = np.random.default_rng(3)
+    reqs = [
+        workloads.small_globule(6000, 1, nq=300, precision="fp32").request,   # K = 128
+        workloads.small_globule(2000, 2, nq=90, precision="fp32").request,    # K = 64
+        workloads.small_globule(3000, 3, nq=120, precision="fp64").request,   # FP64 class
+    ]
+    w = workloads.small_globule(1500, 4, nq=70, precision="fp32").request
+    w.hyd_weights = rng.uniform(0.0, 3.0, w.n_atoms)                      # > 48 weights
+    reqs.append(w)
+    w64 = workloads.small_globule(1200, 5, nq=50, precision="fp64").request
+    w64.hyd_weights = rng.uniform(0.0, 3.0, w64.n_atoms)
+    reqs.append(w64)
+    g = workloads.small_globule(400, 6).globule
+    reqs.append(workloads.grid_solvent_request(g, 0.0, 0.5, 60, "fp32", 1.4))
+    solo = [solve(r, gpu_ctx) for r in reqs]
+    srv = Server(gpu_ctx)
+    for _ in range(2):  # twice, so the second round finds the graphs built
+        tickets = [srv.submit(r) for r in reqs]
+        outs = [srv.wait(t, timeout_s=300) for t in tickets]
+        for a, b in zip(outs, solo):
+            assert np.array_equal(a, b)
