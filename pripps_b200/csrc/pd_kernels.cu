@@ -347,8 +347,6 @@ __device__ __forceinline__ void pairs_range_x2(const float4 *__restrict__ at, in
     SeedGroup<PD_MODE_CLASS, NP, RESID, GENERAL_STEP> cur;
     cur.make(at, jbase, pi, i, ivalid, j0, j1, qs_hi, qs_lo, dq_hi, dq_lo);
     for (int j = j0; j < j1; j += NP) {
-        SeedGroup<PD_MODE_CLASS, NP, RESID, GENERAL_STEP> nxt;  // unused after the last pass
-        nxt.make(at, jbase, pi, i, ivalid, j + NP, j1, qs_hi, qs_lo, dq_hi, dq_lo);
         float2 V[NP], D[NP], NA[NP], WE[NP], WO[NP];
 #pragma unroll
         for (int p = 0; p < NP; ++p) {
@@ -359,6 +357,9 @@ __device__ __forceinline__ void pairs_range_x2(const float4 *__restrict__ at, in
             WO[p] = GENERAL_STEP ? make_float2(cur.S[p].wo, cur.S[p].wo) : WE[p];
         }
         const float2 mvs = make_float2(-cur.vsum, -cur.vsum);
+        // the next pass's seeds (unused after the last pass), computed in
+        // place while the steps below run on this pass's copies
+        cur.make(at, jbase, pi, i, ivalid, j + NP, j1, qs_hi, qs_lo, dq_hi, dq_lo);
         int qoff = 0;  // opaque zero: keeps the K/2 q loads in the loop
         if (RESID) asm volatile("mov.b32 %0, %0;" : "+r"(qoff));
 #pragma unroll
@@ -378,7 +379,6 @@ __device__ __forceinline__ void pairs_range_x2(const float4 *__restrict__ at, in
 #pragma unroll
             for (int p = 0; p < NP; ++p) V[p] = __fadd2_rn(V[p], D[p]);
         }
-        cur = nxt;
     }
 }
 
