@@ -421,6 +421,10 @@ def run_serve(args, ws, rank, local):
     times = [srv.times(t) for t in tickets]
     lat = np.array([d - s for s, a, d in times])
     qwait = np.array([a - s for s, a, d in times])
+    if args.latency_log:
+        np.save(args.latency_log, np.array(
+            [(sr.arrival, a - s, d - s, w.request.n_atoms, w.request.nq)
+             for (s, a, d), sr, w in zip(times, stream, reqs)]))
     pq = sum(w.pair_q for w in reqs)
     check_idx = list(range(0, len(reqs), max(1, len(reqs) // 8)))
     same = all(np.array_equal(outs[i], solve(reqs[i].request, ctx)) for i in check_idx)
@@ -518,6 +522,9 @@ def main():
     ap.add_argument("--requests", type=int, default=200)
     ap.add_argument("--rate", type=float, default=20.0, help="Poisson arrival rate (1/s)")
     ap.add_argument("--budget-gb", type=float, default=40.0)
+    ap.add_argument("--latency-log", default=None,
+                    help="serving: save per-request (arrival s, admission wait s, latency s, "
+                         "n_atoms, nq) to this .npy")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     ws, rank, local = dist_env()

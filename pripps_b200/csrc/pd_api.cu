@@ -1553,8 +1553,8 @@ extern "C" int pd_direct(pd_ctx *ctx, const pd_direct_request *req, double *out)
     if (n == 0 || nv == 0 || req->n_kinds == 0 || !req->xyz || !req->kind || !req->ff ||
         !req->qvec || req->reserved)
         msg = "pd_direct: n_points, n_vectors, n_kinds >= 1 and xyz, kind, ff, qvec required";
-    else if (n > (1ull << 30) || nv > (1ull << 26))
-        msg = "pd_direct: n_points <= 2^30 and n_vectors <= 2^26";
+    else if (n > (1ull << 30) || nv > (1ull << 26) || req->n_kinds > (1u << 24))
+        msg = "pd_direct: n_points <= 2^30, n_vectors <= 2^26 and n_kinds <= 2^24";
     else if (n % nm)
         msg = "box point count (" + std::to_string(n) + ") is not a multiple of the molecule "
               "count (" + std::to_string(nm) + ")";
@@ -1579,9 +1579,11 @@ extern "C" int pd_direct(pd_ctx *ctx, const pd_direct_request *req, double *out)
         return PD_EINVAL;
     }
     const int64_t mol = static_cast<int64_t>(n / nm);
-    const int64_t chunks = pd::direct_chunks(static_cast<int64_t>(n), mol);
-    if (chunks > 65535) {
-        ctx->set_error("pd_direct: too many point chunks for one launch");
+    const int64_t chunks = pd::direct_chunks(static_cast<int64_t>(n), mol, static_cast<int64_t>(nv));
+    if (pd::direct_blocks(static_cast<int64_t>(n), mol, static_cast<int64_t>(nv)) > 0x7fffffffLL ||
+        static_cast<double>(chunks) * static_cast<double>(nv) * 40.0 > 8.0 * (1ull << 30)) {
+        ctx->set_error("pd_direct: points x vectors too large for one call (per-chunk partial "
+                       "amplitudes above 8 GiB); split the q-vectors into batches");
         return PD_EINVAL;
     }
     std::lock_guard<std::mutex> g(ctx->solve_mu);
@@ -1614,8 +1616,9 @@ extern "C" int pd_direct(pd_ctx *ctx, const pd_direct_request *req, double *out)
     if (e == cudaSuccess && d_w)
         e = cudaMemcpyAsync(d_w, req->weight, b_w, cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess)
-        e = pd::launch_direct(d_xyz, d_kind, d_w, d_ff, d_q, static_cast<int64_t>(nv),
-                              static_cast<int64_t>(n), mol, d_part, chunks, d_out, st);
+        e = pd::launch_direct(d_xyz, d_kind, d_w, d_ff, static_cast<int32_t>(req->n_kinds), d_q,
+                              static_cast<int64_t>(nv), static_cast<int64_t>(n), mol, d_part,
+                              chunks, d_out, st);
     if (e == cudaSuccess) {
         ctx->launches += 2;
         e = cudaMemcpyAsync(out, d_out, b_out, cudaMemcpyDeviceToHost, st);

@@ -1012,26 +1012,56 @@ __global__ void pd_stream_accumulate(const double *__restrict__ batch, double sc
 // F(q) = Σ_j f_j(q)·e^{i q·r_j} with q·r evaluated as q_x·x + q_y·y + q_z·z and
 // one sincos per (vector, point). The points are split into chunks that never
 // straddle a molecule: groups of whole molecules (molecules of at most
-// PD_DIRECT_CHUNK points), for which the chunk also forms Σ_m |F_m|², or
-// slices of PD_DIRECT_CHUNK points of one molecule (the last one shorter),
-// whose partial amplitudes the reduction joins per molecule. One thread per
-// q-vector; the chunk's points are read as warp-uniform broadcasts.
-constexpr int PD_DIRECT_CHUNK = 1024;
+// a chunk length of points), for which the chunk also forms Σ_m |F_m|², or
+// slices of that many points of one molecule (the last one shorter), whose
+// partial amplitudes the reduction joins per molecule. The chunk length is
+// 1,024, 512 or 256 points: the longest that still gives PD_DIRECT_BLOCKS
+// blocks, so that the last wave of blocks is a small part of the launch.
+//
+// A block of 128 threads owns 2 × 128 q-vectors (two independent sincos
+// chains per thread) and walks its chunk in stages of PD_DIRECT_STAGE points
+// copied to shared memory (coordinates, weight, kind), which every thread then
+// reads as broadcasts; the form factors of up to PD_DIRECT_SMEM_KINDS kinds for
+// the block's vectors sit in shared memory as well, so the inner loop reads no
+// global memory.
+constexpr int PD_DIRECT_CHUNK_MAX = 1024, PD_DIRECT_CHUNK_MIN = 256;
+constexpr int64_t PD_DIRECT_BLOCKS = 4096;  // about 6 waves of 148 SMs x 5 blocks
+constexpr int PD_DIRECT_THREADS = 128;
+constexpr int PD_DIRECT_V = 2;  // q-vectors per thread
+constexpr int PD_DIRECT_STAGE = 256;
+constexpr int PD_DIRECT_SMEM_KINDS = 16;
 
-__global__ void __launch_bounds__(128) pd_direct_chunks(const double *__restrict__ xyz,
-                                                        const uint32_t *__restrict__ kind,
-                                                        const double *__restrict__ weight,
-                                                        const double *__restrict__ ff,
-                                                        const double *__restrict__ qvec,
-                                                        int64_t n_vec, int64_t mol_size,
-                                                        int64_t chunk_points,
-                                                        int64_t slices_per_mol,
-                                                        int64_t n_points,
-                                                        double *__restrict__ part) {
-    const int64_t v = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
-    const int64_t c = blockIdx.y;
-    if (v >= n_vec) return;
-    const double qx = qvec[3 * v], qy = qvec[3 * v + 1], qz = qvec[3 * v + 2];
+__global__ void __launch_bounds__(PD_DIRECT_THREADS)
+    pd_direct_chunks(const double *__restrict__ xyz, const uint32_t *__restrict__ kind,
+                     const double *__restrict__ weight, const double *__restrict__ ff,
+                     const double *__restrict__ qvec, int64_t n_vec, int64_t n_vblocks,
+                     int64_t mol_size, int64_t chunk_points, int64_t slices_per_mol,
+                     int64_t n_points, int32_t n_kinds, double *__restrict__ part) {
+    constexpr int V = PD_DIRECT_V, T = PD_DIRECT_THREADS;
+    __shared__ double s_x[PD_DIRECT_STAGE], s_y[PD_DIRECT_STAGE], s_z[PD_DIRECT_STAGE],
+        s_w[PD_DIRECT_STAGE];
+    __shared__ uint32_t s_k[PD_DIRECT_STAGE];
+    __shared__ double s_f[PD_DIRECT_SMEM_KINDS][V * T];
+    const int tid = threadIdx.x;
+    // consecutive blocks: the vector blocks of one chunk (its points stay in L2)
+    const int64_t c = blockIdx.x / n_vblocks, vb = blockIdx.x % n_vblocks;
+    int64_t v[V];
+    bool ok[V];
+    double qx[V], qy[V], qz[V];
+#pragma unroll
+    for (int j = 0; j < V; ++j) {
+        v[j] = vb * (V * T) + j * T + tid;
+        ok[j] = v[j] < n_vec;
+        qx[j] = ok[j] ? qvec[3 * v[j]] : 0.0;
+        qy[j] = ok[j] ? qvec[3 * v[j] + 1] : 0.0;
+        qz[j] = ok[j] ? qvec[3 * v[j] + 2] : 0.0;
+    }
+    const bool smem_ff = n_kinds <= PD_DIRECT_SMEM_KINDS;
+    if (smem_ff)
+        for (int k = 0; k < n_kinds; ++k)
+#pragma unroll
+            for (int j = 0; j < V; ++j)
+                s_f[k][j * T + tid] = ok[j] ? ff[static_cast<int64_t>(k) * n_vec + v[j]] : 0.0;
     int64_t p0, p1;
     if (slices_per_mol == 1) {  // whole molecules
         p0 = c * chunk_points;
@@ -1042,61 +1072,115 @@ __global__ void __launch_bounds__(128) pd_direct_chunks(const double *__restrict
         p1 = min((m + 1) * mol_size, p0 + chunk_points);
     }
     const bool whole = slices_per_mol == 1;
-    double ar = 0.0, ai = 0.0, fr = 0.0, fi = 0.0, self = 0.0;
-    for (int64_t p = p0; p < p1; ++p) {
-        const double x = xyz[3 * p], y = xyz[3 * p + 1], z = xyz[3 * p + 2];
-        double f = ff[static_cast<int64_t>(kind[p]) * n_vec + v];
-        if (weight) f = weight[p] * f;  // DummySet::Weighted: w·F
-        const double qr = qx * x + qy * y + qz * z;
-        double sn, cs;
-        sincos(qr, &sn, &cs);
-        fr += f * cs;
-        fi += f * sn;
-        if (whole && (p + 1) % mol_size == 0) {  // a molecule ends inside this chunk
-            ar += fr;
-            ai += fi;
-            self += fr * fr + fi * fi;
-            fr = 0.0;
-            fi = 0.0;
+    int64_t mol_end = (p0 / mol_size + 1) * mol_size;  // first molecule end after p0
+    double ar[V], ai[V], self[V], fr[V], fi[V];
+#pragma unroll
+    for (int j = 0; j < V; ++j) ar[j] = ai[j] = self[j] = fr[j] = fi[j] = 0.0;
+    for (int64_t s0 = p0; s0 < p1; s0 += PD_DIRECT_STAGE) {
+        const int ns = static_cast<int>(min(static_cast<int64_t>(PD_DIRECT_STAGE), p1 - s0));
+        __syncthreads();  // the previous stage is read (and s_f written)
+        for (int t = tid; t < ns; t += T) {
+            const int64_t p = s0 + t;
+            s_x[t] = xyz[3 * p];
+            s_y[t] = xyz[3 * p + 1];
+            s_z[t] = xyz[3 * p + 2];
+            s_w[t] = weight ? weight[p] : 1.0;
+            s_k[t] = kind[p];
         }
-    }
-    // whole molecules: (A, Σ|F_m|²); a slice of a molecule: its open partial F
-    double *o = part + (c * n_vec + v) * 5;
-    o[0] = ar;
-    o[1] = ai;
-    o[2] = self;
-    o[3] = fr;
-    o[4] = fi;
-}
-
-// Per q-vector: A = Σ chunks, Σ_m |F_m|² with the slices of a molecule joined
-// first (chunks in order). out[v] = (Re A, Im A, |A|², Σ_m |F_m|²).
-__global__ void pd_direct_reduce(const double *__restrict__ part, int64_t n_vec, int64_t n_chunks,
-                                 int64_t slices_per_mol, double *__restrict__ out) {
-    const int64_t v = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
-    if (v >= n_vec) return;
-    double ar = 0.0, ai = 0.0, self = 0.0, fr = 0.0, fi = 0.0;
-    for (int64_t c = 0; c < n_chunks; ++c) {
-        const double *o = part + (c * n_vec + v) * 5;
-        ar += o[0];
-        ai += o[1];
-        self += o[2];
-        if (slices_per_mol > 1) {
-            fr += o[3];
-            fi += o[4];
-            if ((c + 1) % slices_per_mol == 0) {
-                ar += fr;
-                ai += fi;
-                self += fr * fr + fi * fi;
-                fr = 0.0;
-                fi = 0.0;
+        __syncthreads();
+        for (int t = 0; t < ns; ++t) {
+            const double x = s_x[t], y = s_y[t], z = s_z[t], w = s_w[t];
+            const uint32_t k = s_k[t];
+#pragma unroll
+            for (int j = 0; j < V; ++j) {
+                double f = smem_ff ? s_f[k][j * T + tid]
+                                   : (ok[j] ? ff[static_cast<int64_t>(k) * n_vec + v[j]] : 0.0);
+                if (weight) f = w * f;  // DummySet::Weighted: w·F
+                const double qr = qx[j] * x + qy[j] * y + qz[j] * z;
+                double sn, cs;
+                sincos(qr, &sn, &cs);
+                fr[j] += f * cs;
+                fi[j] += f * sn;
+            }
+            if (whole && s0 + t + 1 == mol_end) {  // a molecule ends inside this chunk
+#pragma unroll
+                for (int j = 0; j < V; ++j) {
+                    ar[j] += fr[j];
+                    ai[j] += fi[j];
+                    self[j] += fr[j] * fr[j] + fi[j] * fi[j];
+                    fr[j] = 0.0;
+                    fi[j] = 0.0;
+                }
+                mol_end += mol_size;
             }
         }
     }
-    out[4 * v] = ar;
-    out[4 * v + 1] = ai;
-    out[4 * v + 2] = ar * ar + ai * ai;
-    out[4 * v + 3] = self;
+    // whole molecules: (A, Σ|F_m|²); a slice of a molecule: its open partial F
+#pragma unroll
+    for (int j = 0; j < V; ++j) {
+        if (!ok[j]) continue;
+        double *o = part + (c * n_vec + v[j]) * 5;
+        o[0] = ar[j];
+        o[1] = ai[j];
+        o[2] = self[j];
+        o[3] = fr[j];
+        o[4] = fi[j];
+    }
+}
+
+// Per q-vector: A = Σ chunks, Σ_m |F_m|² with the slices of a molecule joined
+// first. out[v] = (Re A, Im A, |A|², Σ_m |F_m|²). A block takes 32 vectors (a
+// lane each); its 8 warps sum 8 fixed runs of whole molecules' chunks, each in
+// chunk order, and the run totals are added in run order: the same sums, in
+// the same order, on every call.
+constexpr int PD_DIRECT_RED_WARPS = 8;
+
+__global__ void __launch_bounds__(32 * PD_DIRECT_RED_WARPS)
+    pd_direct_reduce(const double *__restrict__ part, int64_t n_vec, int64_t n_chunks,
+                     int64_t slices_per_mol, double *__restrict__ out) {
+    __shared__ double s_run[PD_DIRECT_RED_WARPS][3][32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int64_t v = static_cast<int64_t>(blockIdx.x) * 32 + lane;
+    const bool ok = v < n_vec;
+    // runs of whole molecules: chunks [u0·spm, u1·spm)
+    const int64_t units = n_chunks / slices_per_mol;
+    const int64_t u0 = units * w / PD_DIRECT_RED_WARPS, u1 = units * (w + 1) / PD_DIRECT_RED_WARPS;
+    double ar = 0.0, ai = 0.0, self = 0.0, fr = 0.0, fi = 0.0;
+    if (ok) {
+        for (int64_t c = u0 * slices_per_mol; c < u1 * slices_per_mol; ++c) {
+            const double *o = part + (c * n_vec + v) * 5;
+            ar += o[0];
+            ai += o[1];
+            self += o[2];
+            if (slices_per_mol > 1) {
+                fr += o[3];
+                fi += o[4];
+                if ((c + 1) % slices_per_mol == 0) {
+                    ar += fr;
+                    ai += fi;
+                    self += fr * fr + fi * fi;
+                    fr = 0.0;
+                    fi = 0.0;
+                }
+            }
+        }
+    }
+    s_run[w][0][lane] = ar;
+    s_run[w][1][lane] = ai;
+    s_run[w][2][lane] = self;
+    __syncthreads();
+    if (w == 0 && ok) {
+        double a = 0.0, b = 0.0, sf = 0.0;
+        for (int r = 0; r < PD_DIRECT_RED_WARPS; ++r) {
+            a += s_run[r][0][lane];
+            b += s_run[r][1][lane];
+            sf += s_run[r][2][lane];
+        }
+        out[4 * v] = a;
+        out[4 * v + 1] = b;
+        out[4 * v + 2] = a * a + b * b;
+        out[4 * v + 3] = sf;
+    }
 }
 
 // ------------------------------------------------------------ form factors
@@ -1422,40 +1506,54 @@ cudaError_t launch_stream_accumulate(const double *batch, double scale, int32_t 
     return cudaGetLastError();
 }
 
-// Chunking of n_points points in molecules of mol_size: (points per chunk,
-// slices per molecule, number of chunks).
-static void direct_layout(int64_t n_points, int64_t mol_size, int64_t *chunk, int64_t *spm,
-                          int64_t *n_chunks) {
-    if (mol_size <= PD_DIRECT_CHUNK) {
-        *chunk = (PD_DIRECT_CHUNK / mol_size) * mol_size;
-        *spm = 1;
-        *n_chunks = (n_points + *chunk - 1) / *chunk;
-    } else {
-        *chunk = PD_DIRECT_CHUNK;
-        *spm = (mol_size + PD_DIRECT_CHUNK - 1) / PD_DIRECT_CHUNK;
-        *n_chunks = (n_points / mol_size) * *spm;
+// Chunking of n_points points in molecules of mol_size for n_vec vectors:
+// (points per chunk, slices per molecule, number of chunks).
+static void direct_layout(int64_t n_points, int64_t mol_size, int64_t n_vec, int64_t *chunk,
+                          int64_t *spm, int64_t *n_chunks) {
+    const int64_t vblocks = (n_vec + PD_DIRECT_V * PD_DIRECT_THREADS - 1) /
+                            (PD_DIRECT_V * PD_DIRECT_THREADS);
+    for (int64_t len = PD_DIRECT_CHUNK_MAX;; len /= 2) {
+        if (mol_size <= len) {
+            *chunk = (len / mol_size) * mol_size;
+            *spm = 1;
+            *n_chunks = (n_points + *chunk - 1) / *chunk;
+        } else {
+            *chunk = len;
+            *spm = (mol_size + len - 1) / len;
+            *n_chunks = (n_points / mol_size) * *spm;
+        }
+        if (len <= PD_DIRECT_CHUNK_MIN || *n_chunks * vblocks >= PD_DIRECT_BLOCKS) return;
     }
 }
 
-int64_t direct_chunks(int64_t n_points, int64_t mol_size) {
+int64_t direct_chunks(int64_t n_points, int64_t mol_size, int64_t n_vec) {
     int64_t chunk, spm, n;
-    direct_layout(n_points, mol_size, &chunk, &spm, &n);
+    direct_layout(n_points, mol_size, n_vec, &chunk, &spm, &n);
     return n;
 }
 
+int64_t direct_blocks(int64_t n_points, int64_t mol_size, int64_t n_vec) {
+    const int64_t vblocks = (n_vec + PD_DIRECT_V * PD_DIRECT_THREADS - 1) /
+                            (PD_DIRECT_V * PD_DIRECT_THREADS);
+    return direct_chunks(n_points, mol_size, n_vec) * vblocks;
+}
+
 cudaError_t launch_direct(const double *xyz, const uint32_t *kind, const double *weight,
-                          const double *ff, const double *qvec, int64_t n_vec, int64_t n_points,
-                          int64_t mol_size, double *part, int64_t part_chunks, double *out,
-                          cudaStream_t st) {
+                          const double *ff, int32_t n_kinds, const double *qvec, int64_t n_vec,
+                          int64_t n_points, int64_t mol_size, double *part, int64_t part_chunks,
+                          double *out, cudaStream_t st) {
     int64_t chunk, spm, n_chunks;
-    direct_layout(n_points, mol_size, &chunk, &spm, &n_chunks);
-    if (n_chunks > part_chunks || n_chunks > 65535 || n_vec < 1) return cudaErrorInvalidValue;
-    const dim3 g(static_cast<unsigned>((n_vec + 127) / 128), static_cast<unsigned>(n_chunks));
-    pd_direct_chunks<<<g, 128, 0, st>>>(xyz, kind, weight, ff, qvec, n_vec, mol_size, chunk,
-                                        spm, n_points, part);
+    direct_layout(n_points, mol_size, n_vec, &chunk, &spm, &n_chunks);
+    constexpr int64_t per_block = PD_DIRECT_V * PD_DIRECT_THREADS;
+    const int64_t vblocks = (n_vec + per_block - 1) / per_block;
+    if (n_chunks > part_chunks || n_vec < 1 || n_chunks * vblocks > 0x7fffffffLL)
+        return cudaErrorInvalidValue;
+    pd_direct_chunks<<<static_cast<unsigned>(n_chunks * vblocks), PD_DIRECT_THREADS, 0, st>>>(
+        xyz, kind, weight, ff, qvec, n_vec, vblocks, mol_size, chunk, spm, n_points, n_kinds,
+        part);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    pd_direct_reduce<<<static_cast<unsigned>((n_vec + 127) / 128), 128, 0, st>>>(
+    pd_direct_reduce<<<static_cast<unsigned>((n_vec + 31) / 32), 32 * PD_DIRECT_RED_WARPS, 0, st>>>(
         part, n_vec, n_chunks, spm, out);
     return cudaGetLastError();
 }

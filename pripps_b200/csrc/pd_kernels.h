@@ -49,12 +49,14 @@ cudaError_t launch_frame_mean(const double *terms, const double *fw, int32_t n_f
                               double *out, cudaStream_t st, bool normalize = true);
 // Direct transform: (Re A, Im A, |A|², Σ_m |F_m|²) per q-vector for points
 // in molecules of mol_size (n_points a multiple of it). part holds
-// direct_chunks(n_points, mol_size) × n_vec × 5 doubles.
+// direct_chunks(n_points, mol_size, n_vec) × n_vec × 5 doubles; the launch
+// has direct_blocks(…) blocks (at most 2^31 - 1).
 cudaError_t launch_direct(const double *xyz, const uint32_t *kind, const double *weight,
-                          const double *ff, const double *qvec, int64_t n_vec, int64_t n_points,
-                          int64_t mol_size, double *part, int64_t part_chunks, double *out,
-                          cudaStream_t st);
-int64_t direct_chunks(int64_t n_points, int64_t mol_size);
+                          const double *ff, int32_t n_kinds, const double *qvec, int64_t n_vec,
+                          int64_t n_points, int64_t mol_size, double *part, int64_t part_chunks,
+                          double *out, cudaStream_t st);
+int64_t direct_chunks(int64_t n_points, int64_t mol_size, int64_t n_vec);
+int64_t direct_blocks(int64_t n_points, int64_t mol_size, int64_t n_vec);
 // Form-factor tables [n_ff][nq] on the uniform grid; *bad = index + 1 of a
 // form factor whose range misses a grid point (0 if none).
 cudaError_t launch_ff_eval(const int32_t *desc, const double *range, const double *params,

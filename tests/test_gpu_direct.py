@@ -35,6 +35,24 @@ def test_pd_direct_matches_oracle(gpu_ctx, n, n_mol, p_max, weighted):
         assert np.max(np.abs(got[:, c] - ref[:, c]) / scale) < 1e-12, c
 
 
+@pytest.mark.parametrize("n,n_mol,kinds", [(1000, 40, 3), (777, 1, 40), (2100, 7, 17)])
+def test_pd_direct_kinds_and_molecule_ends_across_stages(gpu_ctx, n, n_mol, kinds):
+    """Form factors of more kinds than the kernel keeps in shared memory (read
+    from global memory instead), and molecules that end inside and across the
+    kernel's shared-memory stages of points."""
+    xyz, kind, L = _box(n, n + kinds, kinds=kinds)
+    qv = q_vectors(miller_indices(7), [L, L, L * 1.2])
+    rng = np.random.default_rng(2)
+    ff = rng.uniform(0.5, 8.0, (kinds, len(qv)))
+    w = rng.uniform(0.0, 2.0, n)
+    got = amplitudes(xyz, kind, ff, qv, n_mol, w, gpu_ctx)
+    ref = O.direct_rows(xyz, kind, ff, qv, n_mol, w)
+    fmax = (np.abs(ff).max(axis=0) * np.abs(w).sum()) ** 2
+    for c in range(4):
+        scale = fmax if c >= 2 else np.sqrt(fmax)
+        assert np.max(np.abs(got[:, c] - ref[:, c]) / scale) < 1e-12, c
+
+
 def test_single_molecule_box_and_two_identical_molecules(gpu_ctx):
     """N = 1: S_eff ≡ 1 and P ≡ total; two well-separated identical dumbbells:
     the per-molecule form factor equals the one-molecule intensity
