@@ -538,11 +538,14 @@ struct Lane {
     std::map<std::tuple<int, int, int, int>, cudaGraphExec_t> graphs;  // (precision, K, NP, mode)
 };
 
+#ifndef PD_STEP_COST
+#define PD_STEP_COST 4.0e10
+#endif
 constexpr int STEP_BUFS = 2;       // steps in flight
 constexpr int STEP_LANES = 4;      // kernel variants per step
 constexpr size_t STEP_MAX_JOBS = 1 << 14;
 constexpr size_t STEP_MAX_REQS = 1024;
-constexpr double STEP_COST = 4.0e10;   // ≈ 5 ms of FP32 class-mode work per step
+constexpr double STEP_COST = PD_STEP_COST;  // ≈ 5 ms of FP32 class-mode work per step
 constexpr double RR_QUANTUM = 1.0e9;   // work a request adds per round-robin turn
 
 // Relative cost of one pair·q of a tile (FP32 class mode = 1).
