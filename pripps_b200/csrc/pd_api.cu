@@ -1454,9 +1454,17 @@ int pd_autotune(pd_ctx *ctx, uint64_t n_atoms, uint64_t nq, uint32_t precision) 
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     double *xyz_dev = nullptr, *out_dev = nullptr;
-    cudaMalloc(reinterpret_cast<void **>(&xyz_dev), xyz.size() * 8);
-    cudaMalloc(reinterpret_cast<void **>(&out_dev), 6 * nq * 8);
-    cudaMemcpy(xyz_dev, xyz.data(), xyz.size() * 8, cudaMemcpyHostToDevice);
+    cudaError_t ae = cudaMalloc(reinterpret_cast<void **>(&xyz_dev), xyz.size() * 8);
+    if (ae == cudaSuccess) ae = cudaMalloc(reinterpret_cast<void **>(&out_dev), 6 * nq * 8);
+    if (ae == cudaSuccess)
+        ae = cudaMemcpy(xyz_dev, xyz.data(), xyz.size() * 8, cudaMemcpyHostToDevice);
+    if (ae != cudaSuccess) {
+        cudaFree(xyz_dev);
+        cudaFree(out_dev);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        return cuda_fail(ctx, ae, "pd_autotune");
+    }
     for (auto shape : shapes) {
         const int K = shape.first, NP = shape.second;
         if (precision != PD_FP64 && nq <= 32 && K != 32) continue;
