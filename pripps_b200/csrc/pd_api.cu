@@ -547,6 +547,12 @@ constexpr size_t STEP_MAX_JOBS = 1 << 14;
 constexpr size_t STEP_MAX_REQS = 1024;
 constexpr double STEP_COST = PD_STEP_COST;  // ≈ 5 ms of FP32 class-mode work per step
 constexpr double RR_QUANTUM = 1.0e9;   // work a request adds per round-robin turn
+// Requests of at most this much work (≈1.4 ms alone) skip the steps: at
+// admission their tiles go to an express lane whose stream has the highest
+// priority, so its CTAs take the first SM slots that the running step frees.
+constexpr double EXPRESS_COST = 1.0e10;
+constexpr int EXPRESS = STEP_BUFS;  // row of the express lanes
+static_assert((STEP_BUFS + 1) * STEP_LANES <= 32, "lane bits of PdTicket::used_streams");
 
 // Relative cost of one pair·q of a tile (FP32 class mode = 1).
 double tile_cost(const Plan &P, const PdJob &jb) {
@@ -633,9 +639,11 @@ void worker_main(pd_ctx *ctx) {
     bool init_ok = cudaStreamCreateWithFlags(&sa, cudaStreamNonBlocking) == cudaSuccess &&
                    cudaStreamCreateWithFlags(&sf, cudaStreamNonBlocking) == cudaSuccess &&
                    cudaEventCreateWithFlags(&ev_admit, cudaEventDisableTiming) == cudaSuccess;
-    Lane lanes[STEP_BUFS][STEP_LANES];
-    for (auto &buf : lanes)
-        for (auto &ln : buf) {
+    Lane lanes[STEP_BUFS + 1][STEP_LANES];  // step buffers, then the express row
+    int prio_least = 0, prio_greatest = 0;
+    cudaDeviceGetStreamPriorityRange(&prio_least, &prio_greatest);
+    for (int b = 0; b <= STEP_BUFS; ++b)
+        for (auto &ln : lanes[b]) {
             if (!init_ok) break;
             init_ok &= cudaHostAlloc(reinterpret_cast<void **>(&ln.h_jobs), STEP_MAX_JOBS * sizeof(PdJob), 0) == cudaSuccess;
             init_ok &= cudaHostAlloc(reinterpret_cast<void **>(&ln.h_reqs), STEP_MAX_REQS * sizeof(PdReqDev), 0) == cudaSuccess;
@@ -644,7 +652,9 @@ void worker_main(pd_ctx *ctx) {
             init_ok &= cudaMalloc(reinterpret_cast<void **>(&ln.d_reqs), STEP_MAX_REQS * sizeof(PdReqDev)) == cudaSuccess;
             init_ok &= cudaMalloc(reinterpret_cast<void **>(&ln.d_n), sizeof(int)) == cudaSuccess;
             init_ok &= cudaMalloc(reinterpret_cast<void **>(&ln.d_counter), sizeof(int)) == cudaSuccess;
-            init_ok &= cudaStreamCreateWithFlags(&ln.st, cudaStreamNonBlocking) == cudaSuccess;
+            init_ok &= cudaStreamCreateWithPriority(&ln.st, cudaStreamNonBlocking,
+                                                    b == EXPRESS ? prio_greatest : prio_least) ==
+                       cudaSuccess;
             init_ok &= cudaEventCreateWithFlags(&ln.ev, cudaEventDisableTiming) == cudaSuccess;
         }
     auto lane_of_bit = [&](int bit) -> Lane & { return lanes[bit / STEP_LANES][bit % STEP_LANES]; };
@@ -714,6 +724,7 @@ void worker_main(pd_ctx *ctx) {
         }
         // ---- admission in FIFO order while the budget allows
         bool admitted_now = false;
+        std::vector<std::shared_ptr<PdTicket>> fresh;  // admitted in this pass
         for (auto &t : head) {
             int rc = t->plan_state < 0 ? t->plan_state : PD_OK;
             if (rc == PD_OK) rc = plan_device(ctx, &t->req, t->dp, sa, /*wait=*/true);
@@ -746,11 +757,80 @@ void worker_main(pd_ctx *ctx) {
             t->admitted = true;
             t->t_admit = now_s();
             active.push_back(t);
+            fresh.push_back(t);
             admitted_now = true;
         }
         if (admitted_now) {
             cudaEventRecord(ev_admit, sa);
             admit_recorded = true;
+        }
+
+        // ---- express: small requests admitted now get all their tiles on a
+        // free express lane of their kernel variant (else they take the steps)
+        {
+            Lane *ex = lanes[EXPRESS];
+            std::tuple<int, int, int, int> ex_key[STEP_LANES];
+            std::vector<std::shared_ptr<PdTicket>> ex_members[STEP_LANES];
+            size_t ex_nj[STEP_LANES] = {0, 0, 0, 0};
+            bool ex_used[STEP_LANES] = {false, false, false, false};
+            for (auto &t : fresh) {
+                const Plan &P = t->dp.P;
+                if (t->canceled || t->next_job != 0 || P.jobs.empty()) continue;
+                double cost = 0;
+                for (const PdJob &jb : P.jobs) {
+                    cost += tile_cost(P, jb);
+                    if (cost > EXPRESS_COST) break;
+                }
+                if (cost > EXPRESS_COST) continue;
+                const auto key = std::make_tuple(P.precision, P.tun.K, P.tun.NP, P.mode);
+                int l = -1;
+                for (int c = 0; c < STEP_LANES && l < 0; ++c)
+                    if (ex_used[c] && ex_key[c] == key && ex_nj[c] + P.jobs.size() <= STEP_MAX_JOBS &&
+                        ex_members[c].size() < STEP_MAX_REQS)
+                        l = c;
+                for (int c = 0; c < STEP_LANES && l < 0; ++c) {
+                    if (ex_used[c]) continue;
+                    if (ex[c].busy) {
+                        if (cudaEventQuery(ex[c].ev) != cudaSuccess) continue;
+                        ex[c].busy = false;  // its previous launch (and upload) is done
+                    }
+                    if (P.jobs.size() > STEP_MAX_JOBS) break;
+                    ex_used[c] = true;
+                    ex_key[c] = key;
+                    l = c;
+                }
+                if (l < 0) continue;
+                const int slot = static_cast<int>(ex_members[l].size());
+                ex_members[l].push_back(t);
+                for (; t->next_job < P.jobs.size(); ++t->next_job) {
+                    PdJob jb = P.jobs[t->next_job];
+                    jb.req = slot;
+                    ex[l].h_jobs[ex_nj[l]++] = jb;
+                }
+            }
+            for (int l = 0; l < STEP_LANES; ++l) {
+                if (!ex_used[l]) continue;
+                Lane &ln = ex[l];
+                for (size_t m = 0; m < ex_members[l].size(); ++m)
+                    std::memcpy(&ln.h_reqs[m],
+                                ex_members[l][m]->dp.hptr<char>(ex_members[l][m]->dp.L.req),
+                                sizeof(PdReqDev));
+                *ln.h_n = static_cast<int>(ex_nj[l]);
+                cudaGraphExec_t ge = nullptr;
+                int rc = lane_graph(ctx, ln, std::get<0>(ex_key[l]), std::get<1>(ex_key[l]),
+                                    std::get<2>(ex_key[l]), std::get<3>(ex_key[l]), &ge);
+                if (rc == PD_OK && cudaStreamWaitEvent(ln.st, ev_admit, 0) != cudaSuccess)
+                    rc = PD_EDEVICE;
+                if (rc == PD_OK && cudaGraphLaunch(ge, ln.st) == cudaSuccess &&
+                    cudaEventRecord(ln.ev, ln.st) == cudaSuccess) {
+                    ctx->launches += 1;
+                    ln.busy = true;
+                    const uint32_t bit = 1u << (EXPRESS * STEP_LANES + l);
+                    for (auto &t : ex_members[l]) t->used_streams |= bit;
+                } else {
+                    for (auto &t : ex_members[l]) fail(t, PD_EDEVICE, "express launch failed");
+                }
+            }
         }
 
         // ---- one step: round-robin turns of RR_QUANTUM over the issuable
@@ -760,11 +840,23 @@ void worker_main(pd_ctx *ctx) {
         for (auto &t : active)
             if (!t->canceled && t->next_job < t->dp.P.jobs.size()) cand.push_back(t);
         Lane *step = lanes[cur];
+        // compose into this buffer only once every lane of it is done; the
+        // loop polls instead of waiting, so admission and the express lanes
+        // stay responsive while both buffers run
+        bool buffer_free = true;
+        for (int l = 0; l < STEP_LANES; ++l) {
+            Lane &ln = step[l];
+            if (!ln.busy) continue;
+            if (cudaEventQuery(ln.ev) == cudaSuccess)
+                ln.busy = false;
+            else
+                buffer_free = false;
+        }
         std::tuple<int, int, int, int> lane_key[STEP_LANES];
         std::vector<std::shared_ptr<PdTicket>> members[STEP_LANES];
         size_t nj[STEP_LANES] = {0, 0, 0, 0};
         int n_lanes = 0;
-        if (!cand.empty()) {
+        if (!cand.empty() && buffer_free) {
             std::vector<int> lane_of(cand.size(), -1), slot_of(cand.size(), -1);
             double work = 0;
             bool progress = true;
@@ -843,7 +935,7 @@ void worker_main(pd_ctx *ctx) {
             const bool all_issued = t->next_job >= t->dp.P.jobs.size();
             if (!all_issued && !t->canceled) continue;
             if (admit_recorded) cudaStreamWaitEvent(sf, ev_admit, 0);
-            for (int bit = 0; bit < STEP_BUFS * STEP_LANES; ++bit)
+            for (int bit = 0; bit < (STEP_BUFS + 1) * STEP_LANES; ++bit)
                 if (t->used_streams & (1u << bit)) cudaStreamWaitEvent(sf, lane_of_bit(bit).ev, 0);
             if (t->canceled) {
                 t->drained_only = true;
@@ -905,6 +997,11 @@ void worker_main(pd_ctx *ctx) {
             bool ready = false;
             for (uint64_t id : ctx->pending) ready |= ctx->tickets[id]->plan_state != 0;
             if (!ready && !ctx->stop) ctx->qcv.wait_for(lk, std::chrono::microseconds(200));
+        } else if (issuable && !buffer_free) {
+            // both step buffers busy: poll again in 100 µs, or at once when a
+            // request is submitted or planned
+            std::unique_lock<std::mutex> lk(ctx->qmu);
+            if (!ctx->stop) ctx->qcv.wait_for(lk, std::chrono::microseconds(100));
         }
     }
     sync_all();

@@ -310,6 +310,33 @@ def test_serving_alone_equals_mixed(gpu_ctx):
     assert all(ts[0] <= ts[1] <= ts[2] for ts in times)
 
 
+def test_serving_express_lanes_beside_a_large_request(gpu_ctx):
+    """Small requests (at most 1e10 pair·q of work) submitted while a large
+    one runs go to the high-priority express lanes at admission: more of them,
+    and of more kernel variants, than there are express lanes (the rest take
+    the steps). Every result equals its solo solve bit for bit, and most small
+    requests finish before the large one."""
+    from pripps_b200.serving import Server
+    big = workloads.small_globule(30_000, 11, nq=400).request  # ≈1.8e11 pair·q
+    small = [workloads.small_globule(n, 20 + k, nq=nq, solvent=sol, precision=prec).request
+             for k, (n, nq, sol, prec) in enumerate(
+                 [(4500, 200, True, "fp32"), (1200, 150, False, "fp32"), (800, 40, True, "fp32"),
+                  (2000, 300, True, "fp64"), (6000, 160, True, "fp32"), (500, 500, False, "fp32"),
+                  (3000, 100, True, "fp32"), (1000, 30, True, "fp32"), (2500, 250, False, "fp64"),
+                  (5000, 120, True, "fp32"), (900, 700, True, "fp32"), (1500, 90, False, "fp32")])]
+    solo_big = solve(big, gpu_ctx)
+    solo = [solve(r, gpu_ctx) for r in small]
+    srv = Server(gpu_ctx)
+    tb = srv.submit(big)
+    ts = [srv.submit(r) for r in small]
+    outs = [srv.wait(t, timeout_s=120) for t in ts]
+    assert np.array_equal(srv.wait(tb, timeout_s=120), solo_big)
+    for a, b in zip(outs, solo):
+        assert np.array_equal(a, b)
+    done_big = srv.times(tb)[2]
+    assert sum(srv.times(t)[2] < done_big for t in ts) >= len(ts) // 2
+
+
 def test_serving_budget_admission(gpu_ctx):
     """With a budget that fits about one request, the loop admits them one at
     a time and still completes all; a request that can never fit fails with
