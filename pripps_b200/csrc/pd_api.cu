@@ -840,23 +840,11 @@ void worker_main(pd_ctx *ctx) {
         for (auto &t : active)
             if (!t->canceled && t->next_job < t->dp.P.jobs.size()) cand.push_back(t);
         Lane *step = lanes[cur];
-        // compose into this buffer only once every lane of it is done; the
-        // loop polls instead of waiting, so admission and the express lanes
-        // stay responsive while both buffers run
-        bool buffer_free = true;
-        for (int l = 0; l < STEP_LANES; ++l) {
-            Lane &ln = step[l];
-            if (!ln.busy) continue;
-            if (cudaEventQuery(ln.ev) == cudaSuccess)
-                ln.busy = false;
-            else
-                buffer_free = false;
-        }
         std::tuple<int, int, int, int> lane_key[STEP_LANES];
         std::vector<std::shared_ptr<PdTicket>> members[STEP_LANES];
         size_t nj[STEP_LANES] = {0, 0, 0, 0};
         int n_lanes = 0;
-        if (!cand.empty() && buffer_free) {
+        if (!cand.empty()) {
             std::vector<int> lane_of(cand.size(), -1), slot_of(cand.size(), -1);
             double work = 0;
             bool progress = true;
@@ -875,8 +863,11 @@ void worker_main(pd_ctx *ctx) {
                         if (l == n_lanes) {
                             if (n_lanes == STEP_LANES) continue;  // next step
                             Lane &ln = step[l];
-                            if (ln.busy) {  // its previous upload may still read h_*
-                                cudaEventSynchronize(ln.ev);
+                            // a lane still running its previous step is not
+                            // waited for (the loop polls again): its request
+                            // and any new variant take a later step
+                            if (ln.busy) {
+                                if (cudaEventQuery(ln.ev) != cudaSuccess) continue;
                                 ln.busy = false;
                             }
                             lane_key[n_lanes++] = key;
@@ -997,9 +988,9 @@ void worker_main(pd_ctx *ctx) {
             bool ready = false;
             for (uint64_t id : ctx->pending) ready |= ctx->tickets[id]->plan_state != 0;
             if (!ready && !ctx->stop) ctx->qcv.wait_for(lk, std::chrono::microseconds(200));
-        } else if (issuable && !buffer_free) {
-            // both step buffers busy: poll again in 100 µs, or at once when a
-            // request is submitted or planned
+        } else if (issuable && n_lanes == 0) {
+            // no lane of the step buffer was free: poll again in 100 µs, or at
+            // once when a request is submitted or planned
             std::unique_lock<std::mutex> lk(ctx->qmu);
             if (!ctx->stop) ctx->qcv.wait_for(lk, std::chrono::microseconds(100));
         }
