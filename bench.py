@@ -467,10 +467,11 @@ def run_serve(args, ws, rank, local):
 
 
 def run_direct(args, ws, rank, local):
-    """Direct transform of a periodic box (pd_direct): 64 copies of a
-    2,000-atom globule on a 4×4×4 grid in a 320 Å box, Miller vectors with
-    p_max = args.p_max, per-molecule self terms. Unit: (q-vector, point)
-    amplitude terms per second; the oracle's rows on a sample beside it."""
+    """Direct transform of a periodic box (pd_direct_lattice, with pd_direct
+    beside it): 64 copies of a 2,000-atom globule on a 4×4×4 grid in a 320 Å
+    box, Miller vectors with p_max = args.p_max, per-molecule self terms.
+    Unit: (q-vector, point) amplitude terms per second; the oracle's rows on a
+    sample beside it."""
     import torch
     from oracle import oracle as O
     from pripps_b200 import _lib, synth, workloads
@@ -484,18 +485,29 @@ def run_direct(args, ws, rank, local):
     ids = workloads.element_ids()[np.tile(g.elements, len(offs))]
     used = np.unique(ids)
     kind = np.searchsorted(used, ids)
-    qv = q_vectors(miller_indices(args.p_max), [L] * 3)
+    hkl = miller_indices(args.p_max)
+    qv = q_vectors(hkl, [L] * 3)
     qn = np.sqrt((qv * qv).sum(axis=1))
     ff = workloads.foxs().table(used, qn)
-    for _ in range(args.warmup):
-        amplitudes(xyz, kind, ff, qv, len(offs), None, ctx)
-    times = []
-    for _ in range(args.steps):
-        t0 = time.perf_counter()
-        rows = amplitudes(xyz, kind, ff, qv, len(offs), None, ctx)
-        times.append(time.perf_counter() - t0)
+
+    def run(lattice):
+        if lattice:  # pd_direct_lattice: per-point phase tables (the path DirectTransform takes)
+            return amplitudes(xyz, kind, ff, None, len(offs), None, ctx, hkl=hkl, box=[L] * 3)
+        return amplitudes(xyz, kind, ff, qv, len(offs), None, ctx)  # pd_direct: one sincos per term
+
+    def timed(lattice):
+        for _ in range(args.warmup):
+            run(lattice)
+        ts = []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            r = run(lattice)
+            ts.append(time.perf_counter() - t0)
+        return 1e3 * sum(ts) / len(ts), r
+
+    ms, rows = timed(True)
+    ms_sincos, rows_sincos = timed(False)
     work = len(qv) * len(xyz)
-    ms = 1e3 * sum(times) / len(times)
     # oracle on a sample: the first 8 molecules (16,000 points), 39 vectors
     nsamp = 16000
     t0 = time.perf_counter()
@@ -509,7 +521,13 @@ def run_direct(args, ws, rank, local):
             "dtype": "f64", "data": "synthetic",
             "config": {"workload": "direct_box_64x2000", "points": len(xyz), "molecules": 64,
                        "box": L, "p_max": args.p_max, "vectors": len(qv),
-                       "timed": "blocking pd_direct with host buffers (upload, kernels, download)"},
+                       "timed": "blocking pd_direct_lattice with host buffers (upload, "
+                                "phase tables + amplitude kernel, reduction, download)"},
+            "sincos_path": {"value": work / (ms_sincos * 1e-3), "ms_per_step": ms_sincos,
+                            "entry": "pd_direct (one FP64 sincos per term)",
+                            "max_rel_diff_self_term": float(np.max(
+                                np.abs(rows[:, 3] - rows_sincos[:, 3]) /
+                                np.abs(rows_sincos[:, 3]).max()))},
             "cpu_baseline": {"value": nsamp * 39 / dt, "unit": "vector·point/s", "cores": 1,
                              "kind": "port", "sample": "16,000 points x 39 vectors",
                              "seconds": dt},

@@ -236,6 +236,15 @@ typedef struct pd_direct_request {
                                   (DummySet::Weighted, src/solvent/mod.rs:365-371) */
 } pd_direct_request;
 int pd_direct(pd_ctx *ctx, const pd_direct_request *req, double *out);
+/* The same rows at reciprocal-lattice vectors q = 2π·(h, k, l)/box, given as
+ * integer indices hkl [n_vectors][3] (req->qvec is not read; ff columns follow
+ * the hkl rows). Each term's phase comes from per-point tables of
+ * e^{i2πn·x_a/L_a}, n = 0..max|index| (negative n by conjugation), built on
+ * the device — the reference's PhaseTable (src/explicit.rs:85-135) — instead
+ * of a sincos; indices beyond 512 take the sincos kernel at q = 2π·hkl/box.
+ * Within 1e-12 of pd_direct at the same vectors. box sides finite and > 0. */
+int pd_direct_lattice(pd_ctx *ctx, const pd_direct_request *req, const int32_t *hkl,
+                      const double box[3], double *out);
 
 /* Form factors evaluated on the device: the reference's FormFactor kinds
  * (src/formfactor.rs:130-201; United is a 101-point Table after loading,

@@ -126,6 +126,8 @@ SIGNATURES = {
     "pd_launch_count": (C.c_uint64, [_P]),
     "pd_solve_noalloc": (C.c_int, [C.POINTER(PdRequest), C.c_void_p, C.c_void_p, C.c_void_p]),
     "pd_direct": (C.c_int, [_P, C.POINTER(PdDirectRequest), _D]),
+    "pd_direct_lattice": (C.c_int, [_P, C.POINTER(PdDirectRequest), C.POINTER(C.c_int32), _D,
+                                    _D]),
     "pd_formfactor_tables": (C.c_int, [_P, C.POINTER(PdFormFactor), C.c_uint32, C.c_double,
                                        C.c_double, C.c_uint64, _D]),
     "pd_stream_open": (C.c_int, [_P, C.POINTER(PdRequest), C.c_uint32, C.POINTER(_P)]),

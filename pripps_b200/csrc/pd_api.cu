@@ -8,6 +8,7 @@
 #include <atomic>
 #include <chrono>
 #include <cmath>
+#include <cstdlib>
 #include <condition_variable>
 #include <cstdio>
 #include <cstring>
@@ -1644,39 +1645,40 @@ uint64_t pd_launch_count(pd_ctx *ctx) { return ctx ? ctx->launches.load() : 0; }
 }  // extern "C"
 
 // ---------------------------------------------------------------- direct transform
-extern "C" int pd_direct(pd_ctx *ctx, const pd_direct_request *req, double *out) {
-    if (!ctx || !req || !out) return PD_EINVAL;
+namespace {
+
+// Checks shared by pd_direct and pd_direct_lattice (the q-vectors apart).
+std::string direct_validate(const pd_direct_request *req) {
     const uint64_t n = req->n_points, nv = req->n_vectors;
     const uint64_t nm = req->n_molecules ? req->n_molecules : 1;
-    std::string msg;
     if (n == 0 || nv == 0 || req->n_kinds == 0 || !req->xyz || !req->kind || !req->ff ||
-        !req->qvec || req->reserved)
-        msg = "pd_direct: n_points, n_vectors, n_kinds >= 1 and xyz, kind, ff, qvec required";
-    else if (n > (1ull << 30) || nv > (1ull << 26) || req->n_kinds > (1u << 24))
-        msg = "pd_direct: n_points <= 2^30, n_vectors <= 2^26 and n_kinds <= 2^24";
-    else if (n % nm)
-        msg = "box point count (" + std::to_string(n) + ") is not a multiple of the molecule "
-              "count (" + std::to_string(nm) + ")";
-    if (msg.empty()) {
-        for (uint64_t i = 0; i < n; ++i)
-            if (req->kind[i] >= req->n_kinds) {
-                msg = "kind " + std::to_string(req->kind[i]) + " at point " + std::to_string(i) +
-                      " is >= n_kinds";
-                break;
-            }
-        for (uint64_t i = 0; msg.empty() && i < 3 * n; ++i)
-            if (!std::isfinite(req->xyz[i])) msg = "non-finite coordinate";
-        for (uint64_t i = 0; msg.empty() && i < 3 * nv; ++i)
-            if (!std::isfinite(req->qvec[i])) msg = "non-finite q-vector";
-        for (uint64_t i = 0; msg.empty() && i < nv * req->n_kinds; ++i)
-            if (!std::isfinite(req->ff[i])) msg = "non-finite form factor";
-        for (uint64_t i = 0; msg.empty() && req->weight && i < n; ++i)
-            if (!std::isfinite(req->weight[i])) msg = "non-finite point weight";
-    }
-    if (!msg.empty()) {
-        ctx->set_error(msg);
-        return PD_EINVAL;
-    }
+        req->reserved)
+        return "pd_direct: n_points, n_vectors, n_kinds >= 1 and xyz, kind, ff required";
+    if (n > (1ull << 30) || nv > (1ull << 26) || req->n_kinds > (1u << 24))
+        return "pd_direct: n_points <= 2^30, n_vectors <= 2^26 and n_kinds <= 2^24";
+    if (n % nm)
+        return "box point count (" + std::to_string(n) + ") is not a multiple of the molecule "
+               "count (" + std::to_string(nm) + ")";
+    for (uint64_t i = 0; i < n; ++i)
+        if (req->kind[i] >= req->n_kinds)
+            return "kind " + std::to_string(req->kind[i]) + " at point " + std::to_string(i) +
+                   " is >= n_kinds";
+    for (uint64_t i = 0; i < 3 * n; ++i)
+        if (!std::isfinite(req->xyz[i])) return "non-finite coordinate";
+    for (uint64_t i = 0; i < nv * req->n_kinds; ++i)
+        if (!std::isfinite(req->ff[i])) return "non-finite form factor";
+    for (uint64_t i = 0; req->weight && i < n; ++i)
+        if (!std::isfinite(req->weight[i])) return "non-finite point weight";
+    return std::string();
+}
+
+// One blocking Direct solve: either explicit q-vectors (qvec, the sincos
+// kernel) or lattice indices (hkl with |index| <= nmax and box, the phase-table
+// kernel). ff is [n_kinds][n_vectors] in the order of the vectors given.
+int direct_run(pd_ctx *ctx, const pd_direct_request *req, const double *ff, const double *qvec,
+               const int32_t *hkl, int32_t nmax, const double *box, double *out) {
+    const uint64_t n = req->n_points, nv = req->n_vectors;
+    const uint64_t nm = req->n_molecules ? req->n_molecules : 1;
     const int64_t mol = static_cast<int64_t>(n / nm);
     const int64_t chunks = pd::direct_chunks(static_cast<int64_t>(n), mol, static_cast<int64_t>(nv));
     if (pd::direct_blocks(static_cast<int64_t>(n), mol, static_cast<int64_t>(nv)) > 0x7fffffffLL ||
@@ -1688,9 +1690,9 @@ extern "C" int pd_direct(pd_ctx *ctx, const pd_direct_request *req, double *out)
     std::lock_guard<std::mutex> g(ctx->solve_mu);
     cudaSetDevice(ctx->device);
     cudaStream_t st = ctx->stream;
-    const size_t b_xyz = n * 24, b_kind = n * 4, b_ff = nv * req->n_kinds * 8, b_q = nv * 24,
-                 b_part = static_cast<size_t>(chunks) * nv * 40, b_out = nv * 32,
-                 b_w = req->weight ? n * 8 : 0;
+    const size_t b_xyz = n * 24, b_kind = n * 4, b_ff = nv * req->n_kinds * 8,
+                 b_q = hkl ? nv * 12 : nv * 24, b_part = static_cast<size_t>(chunks) * nv * 40,
+                 b_out = nv * 32, b_w = req->weight ? n * 8 : 0;
     const size_t total = align_up(b_xyz, 256) + align_up(b_kind, 256) + align_up(b_ff, 256) +
                          align_up(b_q, 256) + align_up(b_part, 256) + align_up(b_w, 256) + b_out;
     char *base = nullptr;
@@ -1704,20 +1706,28 @@ extern "C" int pd_direct(pd_ctx *ctx, const pd_direct_request *req, double *out)
     double *d_xyz = reinterpret_cast<double *>(take(b_xyz));
     uint32_t *d_kind = reinterpret_cast<uint32_t *>(take(b_kind));
     double *d_ff = reinterpret_cast<double *>(take(b_ff));
-    double *d_q = reinterpret_cast<double *>(take(b_q));
+    char *d_q = take(b_q);
     double *d_part = reinterpret_cast<double *>(take(b_part));
     double *d_w = req->weight ? reinterpret_cast<double *>(take(b_w)) : nullptr;
     double *d_out = reinterpret_cast<double *>(take(b_out));
     cudaError_t e = cudaMemcpyAsync(d_xyz, req->xyz, b_xyz, cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(d_kind, req->kind, b_kind, cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(d_ff, req->ff, b_ff, cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(d_q, req->qvec, b_q, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_ff, ff, b_ff, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(d_q, hkl ? static_cast<const void *>(hkl) : qvec, b_q,
+                            cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess && d_w)
         e = cudaMemcpyAsync(d_w, req->weight, b_w, cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess)
-        e = pd::launch_direct(d_xyz, d_kind, d_w, d_ff, static_cast<int32_t>(req->n_kinds), d_q,
-                              static_cast<int64_t>(nv), static_cast<int64_t>(n), mol, d_part,
-                              chunks, d_out, st);
+    if (e == cudaSuccess) {
+        if (hkl)
+            e = pd::launch_direct_table(d_xyz, d_kind, d_w, d_ff, reinterpret_cast<int32_t *>(d_q),
+                                        nmax, box, static_cast<int64_t>(nv),
+                                        static_cast<int64_t>(n), mol, d_part, chunks, d_out, st);
+        else
+            e = pd::launch_direct(d_xyz, d_kind, d_w, d_ff, static_cast<int32_t>(req->n_kinds),
+                                  reinterpret_cast<double *>(d_q), static_cast<int64_t>(nv),
+                                  static_cast<int64_t>(n), mol, d_part, chunks, d_out, st);
+    }
     if (e == cudaSuccess) {
         ctx->launches += 2;
         e = cudaMemcpyAsync(out, d_out, b_out, cudaMemcpyDeviceToHost, st);
@@ -1726,6 +1736,66 @@ extern "C" int pd_direct(pd_ctx *ctx, const pd_direct_request *req, double *out)
     const cudaError_t e2 = cudaStreamSynchronize(st);
     if (e == cudaSuccess) e = e2;
     if (e != cudaSuccess) return cuda_fail(ctx, e, "pd_direct");
+    return PD_OK;
+}
+
+// Lattice indices up to this bound use the phase tables; beyond it a table
+// row costs more than the sincos it saves, and the vectors go to the sincos
+// kernel as q = 2π·hkl/L.
+constexpr int64_t kDirectTableMaxIndex = 512;
+
+}  // namespace
+
+extern "C" int pd_direct(pd_ctx *ctx, const pd_direct_request *req, double *out) {
+    if (!ctx || !req || !out) return PD_EINVAL;
+    std::string msg = req->qvec ? direct_validate(req) : "pd_direct: qvec required";
+    for (uint64_t i = 0; msg.empty() && i < 3 * req->n_vectors; ++i)
+        if (!std::isfinite(req->qvec[i])) msg = "non-finite q-vector";
+    if (!msg.empty()) {
+        ctx->set_error(msg);
+        return PD_EINVAL;
+    }
+    return direct_run(ctx, req, req->ff, req->qvec, nullptr, 0, nullptr, out);
+}
+
+extern "C" int pd_direct_lattice(pd_ctx *ctx, const pd_direct_request *req, const int32_t *hkl,
+                                 const double box[3], double *out) {
+    if (!ctx || !req || !out) return PD_EINVAL;
+    std::string msg = (hkl && box) ? direct_validate(req) : "pd_direct_lattice: hkl and box required";
+    for (int a = 0; msg.empty() && a < 3; ++a)
+        if (!std::isfinite(box[a]) || !(box[a] > 0.0)) msg = "box sides must be finite and > 0";
+    if (!msg.empty()) {
+        ctx->set_error(msg);
+        return PD_EINVAL;
+    }
+    const uint64_t nv = req->n_vectors, nk = req->n_kinds;
+    int64_t nmax = 0;
+    for (uint64_t i = 0; i < 3 * nv; ++i)
+        nmax = std::max<int64_t>(nmax, std::llabs(static_cast<long long>(hkl[i])));
+    if (nmax > kDirectTableMaxIndex || pd::direct_table_points(static_cast<int32_t>(nmax)) < 1) {
+        std::vector<double> q(3 * nv);
+        for (uint64_t i = 0; i < nv; ++i)
+            for (int a = 0; a < 3; ++a)
+                q[3 * i + a] = (2.0 * M_PI * static_cast<double>(hkl[3 * i + a])) / box[a];
+        return direct_run(ctx, req, req->ff, q.data(), nullptr, 0, nullptr, out);
+    }
+    // vectors in (h, k, l) order, so that a warp's table reads share rows
+    std::vector<uint32_t> perm(nv);
+    for (uint64_t i = 0; i < nv; ++i) perm[i] = static_cast<uint32_t>(i);
+    std::stable_sort(perm.begin(), perm.end(), [&](uint32_t x, uint32_t y) {
+        return std::lexicographical_compare(hkl + 3 * x, hkl + 3 * x + 3, hkl + 3 * y, hkl + 3 * y + 3);
+    });
+    std::vector<int32_t> hs(3 * nv);
+    std::vector<double> fs(nk * nv), os(4 * nv);
+    for (uint64_t i = 0; i < nv; ++i) {
+        for (int a = 0; a < 3; ++a) hs[3 * i + a] = hkl[3 * perm[i] + a];
+        for (uint64_t k = 0; k < nk; ++k) fs[k * nv + i] = req->ff[k * nv + perm[i]];
+    }
+    const int rc = direct_run(ctx, req, fs.data(), nullptr, hs.data(), static_cast<int32_t>(nmax),
+                              box, os.data());
+    if (rc != PD_OK) return rc;
+    for (uint64_t i = 0; i < nv; ++i)
+        for (int c = 0; c < 4; ++c) out[4 * perm[i] + c] = os[4 * i + c];
     return PD_OK;
 }
 

@@ -20,6 +20,7 @@
 // every pair and q, and FP64 accumulation throughout.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <atomic>
 #include <cstdint>
 #include <cstdio>
@@ -1128,6 +1129,131 @@ __global__ void __launch_bounds__(PD_DIRECT_THREADS)
     }
 }
 
+// Direct transform at reciprocal-lattice vectors q = 2π·(h, k, l)/L: the phase
+// of a term is e^{i2πh·x/Lx}·e^{i2πk·y/Ly}·e^{i2πl·z/Lz}. Per stage of points
+// the block builds, in shared memory, each point's powers e^{i2πn·x_a/L_a} for
+// n = 0..nmax on every axis (e^{i2π·x_a/L_a} from one sincos, then successive
+// products, negative n by conjugation: the reference's PhaseTable,
+// src/explicit.rs:85-135). A term then costs three table reads and two
+// complex products instead of a sincos. Same chunks, partial layout and
+// reduction as pd_direct_chunks; 256 threads own 3 × 256 vectors.
+constexpr int PD_DTAB_THREADS = 256;
+constexpr int PD_DTAB_V = 3;
+constexpr int PD_DTAB_MAX_POINTS = 64;
+constexpr int PD_DTAB_TABLE_BYTES = 96 * 1024;
+
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+    return make_double2(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
+}
+// a, or its conjugate when neg is the sign bit of the high word
+__device__ __forceinline__ double2 conj_if(double2 a, int neg) {
+    return make_double2(a.x, __hiloint2double(__double2hiint(a.y) ^ neg, __double2loint(a.y)));
+}
+
+__global__ void __launch_bounds__(PD_DTAB_THREADS, 2)
+    pd_direct_table(const double *__restrict__ xyz, const uint32_t *__restrict__ kind,
+                    const double *__restrict__ weight, const double *__restrict__ ff,
+                    const int32_t *__restrict__ hkl, double lx, double ly, double lz,
+                    int32_t stride, int32_t npts, int64_t n_vec, int64_t n_vblocks,
+                    int64_t mol_size, int64_t chunk_points, int64_t slices_per_mol,
+                    int64_t n_points, double *__restrict__ part) {
+    constexpr int V = PD_DTAB_V, T = PD_DTAB_THREADS;
+    extern __shared__ __align__(16) double2 pd_dtab[];  // [npts][3][stride]
+    __shared__ double s_w[PD_DTAB_MAX_POINTS];
+    __shared__ uint32_t s_k[PD_DTAB_MAX_POINTS];
+    const int tid = threadIdx.x;
+    const int64_t c = blockIdx.x / n_vblocks, vb = blockIdx.x % n_vblocks;
+    int64_t v[V];
+    bool ok[V];
+    int ox[V], oy[V], oz[V], sx[V], sy[V], sz[V];
+#pragma unroll
+    for (int j = 0; j < V; ++j) {
+        v[j] = vb * (V * T) + j * T + tid;
+        ok[j] = v[j] < n_vec;
+        const int h = ok[j] ? hkl[3 * v[j]] : 0, k = ok[j] ? hkl[3 * v[j] + 1] : 0,
+                  l = ok[j] ? hkl[3 * v[j] + 2] : 0;
+        ox[j] = abs(h);
+        oy[j] = stride + abs(k);
+        oz[j] = 2 * stride + abs(l);
+        sx[j] = h < 0 ? static_cast<int>(0x80000000u) : 0;
+        sy[j] = k < 0 ? static_cast<int>(0x80000000u) : 0;
+        sz[j] = l < 0 ? static_cast<int>(0x80000000u) : 0;
+    }
+    int64_t p0, p1;
+    if (slices_per_mol == 1) {
+        p0 = c * chunk_points;
+        p1 = min(n_points, p0 + chunk_points);
+    } else {
+        const int64_t m = c / slices_per_mol, sl = c % slices_per_mol;
+        p0 = m * mol_size + sl * chunk_points;
+        p1 = min((m + 1) * mol_size, p0 + chunk_points);
+    }
+    const bool whole = slices_per_mol == 1;
+    int64_t mol_end = (p0 / mol_size + 1) * mol_size;
+    double ar[V], ai[V], self[V], fr[V], fi[V];
+#pragma unroll
+    for (int j = 0; j < V; ++j) ar[j] = ai[j] = self[j] = fr[j] = fi[j] = 0.0;
+    for (int64_t s0 = p0; s0 < p1; s0 += npts) {
+        const int ns = static_cast<int>(min(static_cast<int64_t>(npts), p1 - s0));
+        __syncthreads();  // the previous stage's table is read
+        // one thread per (point, axis): the row e^{i2πn·x_a/L_a}, n = 0..stride-1
+        for (int t = tid; t < 3 * ns; t += T) {
+            const int pt = t / 3, a = t - 3 * pt;
+            const double x = xyz[3 * (s0 + pt) + a];
+            const double L = a == 0 ? lx : (a == 1 ? ly : lz);
+            double sn, cs;
+            sincos(2.0 * 3.141592653589793 * x / L, &sn, &cs);
+            const double2 step = make_double2(cs, sn);
+            double2 e = make_double2(1.0, 0.0);
+            double2 *row = pd_dtab + (3 * pt + a) * stride;
+            for (int n = 0; n < stride; ++n) {
+                row[n] = e;
+                e = cmul(e, step);
+            }
+        }
+        for (int t = tid; t < ns; t += T) {
+            s_w[t] = weight ? weight[s0 + t] : 1.0;
+            s_k[t] = kind[s0 + t];
+        }
+        __syncthreads();
+        for (int pt = 0; pt < ns; ++pt) {
+            const double2 *row = pd_dtab + 3 * pt * stride;
+            const double w = s_w[pt];
+            const uint32_t k = s_k[pt];
+#pragma unroll
+            for (int j = 0; j < V; ++j) {
+                double f = ok[j] ? ff[static_cast<int64_t>(k) * n_vec + v[j]] : 0.0;
+                if (weight) f = w * f;  // DummySet::Weighted: w·F
+                const double2 ph = cmul(cmul(conj_if(row[ox[j]], sx[j]), conj_if(row[oy[j]], sy[j])),
+                                        conj_if(row[oz[j]], sz[j]));
+                fr[j] += f * ph.x;
+                fi[j] += f * ph.y;
+            }
+            if (whole && s0 + pt + 1 == mol_end) {
+#pragma unroll
+                for (int j = 0; j < V; ++j) {
+                    ar[j] += fr[j];
+                    ai[j] += fi[j];
+                    self[j] += fr[j] * fr[j] + fi[j] * fi[j];
+                    fr[j] = 0.0;
+                    fi[j] = 0.0;
+                }
+                mol_end += mol_size;
+            }
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < V; ++j) {
+        if (!ok[j]) continue;
+        double *o = part + (c * n_vec + v[j]) * 5;
+        o[0] = ar[j];
+        o[1] = ai[j];
+        o[2] = self[j];
+        o[3] = fr[j];
+        o[4] = fi[j];
+    }
+}
+
 // Per q-vector: A = Σ chunks, Σ_m |F_m|² with the slices of a molecule joined
 // first. out[v] = (Re A, Im A, |A|², Σ_m |F_m|²). A block takes 32 vectors (a
 // lane each); its 8 warps sum 8 fixed runs of whole molecules' chunks, each in
@@ -1551,6 +1677,48 @@ cudaError_t launch_direct(const double *xyz, const uint32_t *kind, const double 
     pd_direct_chunks<<<static_cast<unsigned>(n_chunks * vblocks), PD_DIRECT_THREADS, 0, st>>>(
         xyz, kind, weight, ff, qvec, n_vec, vblocks, mol_size, chunk, spm, n_points, n_kinds,
         part);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    pd_direct_reduce<<<static_cast<unsigned>((n_vec + 31) / 32), 32 * PD_DIRECT_RED_WARPS, 0, st>>>(
+        part, n_vec, n_chunks, spm, out);
+    return cudaGetLastError();
+}
+
+// Stage length of the table kernel for indices up to nmax (0 when a single
+// point's table does not fit).
+int direct_table_points(int32_t nmax) {
+    const int64_t per_point = 3LL * (nmax + 1) * static_cast<int64_t>(sizeof(double2));
+    return static_cast<int>(std::min<int64_t>(PD_DTAB_MAX_POINTS, PD_DTAB_TABLE_BYTES / per_point));
+}
+
+cudaError_t launch_direct_table(const double *xyz, const uint32_t *kind, const double *weight,
+                                const double *ff, const int32_t *hkl, int32_t nmax,
+                                const double box[3], int64_t n_vec, int64_t n_points,
+                                int64_t mol_size, double *part, int64_t part_chunks, double *out,
+                                cudaStream_t st) {
+    const int npts = direct_table_points(nmax);
+    if (npts < 1 || n_vec < 1) return cudaErrorInvalidValue;
+    const int stride = nmax + 1;
+    const size_t smem = static_cast<size_t>(npts) * 3 * stride * sizeof(double2);
+    // above 48 KB of dynamic shared memory needs the opt-in, set once per device
+    static std::atomic<uint64_t> done{0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const uint64_t bit = dev < 64 ? (uint64_t{1} << dev) : 0;
+    if (!bit || !(done.load() & bit)) {
+        const cudaError_t e = cudaFuncSetAttribute(
+            pd_direct_table, cudaFuncAttributeMaxDynamicSharedMemorySize, PD_DTAB_TABLE_BYTES);
+        if (e != cudaSuccess) return e;
+        if (bit) done.fetch_or(bit);
+    }
+    int64_t chunk, spm, n_chunks;
+    direct_layout(n_points, mol_size, n_vec, &chunk, &spm, &n_chunks);
+    constexpr int64_t per_block = PD_DTAB_V * PD_DTAB_THREADS;
+    const int64_t vblocks = (n_vec + per_block - 1) / per_block;
+    if (n_chunks > part_chunks || n_chunks * vblocks > 0x7fffffffLL) return cudaErrorInvalidValue;
+    pd_direct_table<<<static_cast<unsigned>(n_chunks * vblocks), PD_DTAB_THREADS, smem, st>>>(
+        xyz, kind, weight, ff, hkl, box[0], box[1], box[2], stride, npts, n_vec, vblocks,
+        mol_size, chunk, spm, n_points, part);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     pd_direct_reduce<<<static_cast<unsigned>((n_vec + 31) / 32), 32 * PD_DIRECT_RED_WARPS, 0, st>>>(

@@ -56,6 +56,15 @@ cudaError_t launch_direct(const double *xyz, const uint32_t *kind, const double 
                           int64_t n_points, int64_t mol_size, double *part, int64_t part_chunks,
                           double *out, cudaStream_t st);
 int64_t direct_chunks(int64_t n_points, int64_t mol_size, int64_t n_vec);
+// Direct transform at lattice vectors q = 2π·hkl/box from per-point phase
+// tables (indices |h|, |k|, |l| <= nmax, with direct_table_points(nmax) >= 1);
+// same part and out layouts as launch_direct.
+int direct_table_points(int32_t nmax);
+cudaError_t launch_direct_table(const double *xyz, const uint32_t *kind, const double *weight,
+                                const double *ff, const int32_t *hkl, int32_t nmax,
+                                const double box[3], int64_t n_vec, int64_t n_points,
+                                int64_t mol_size, double *part, int64_t part_chunks, double *out,
+                                cudaStream_t st);
 int64_t direct_blocks(int64_t n_points, int64_t mol_size, int64_t n_vec);
 // Form-factor tables [n_ff][nq] on the uniform grid; *bad = index + 1 of a
 // form factor whose range misses a grid point (0 if none).

@@ -81,15 +81,28 @@ def average_by_qnorm(qs: np.ndarray, values: np.ndarray):
     return np.array([out_q[k] for k in order]), np.array([out_v[k] for k in order])
 
 
-def amplitudes(xyz: np.ndarray, kind: np.ndarray, ff: np.ndarray, qvec: np.ndarray,
+def amplitudes(xyz: np.ndarray, kind: np.ndarray, ff: np.ndarray, qvec: Optional[np.ndarray],
                n_molecules: int = 1, weight: Optional[np.ndarray] = None,
-               ctx: Optional[_lib.Context] = None) -> np.ndarray:
-    """pd_direct: [n_vectors, 4] = (Re A, Im A, |A|², Σ_m |F_m|²)."""
+               ctx: Optional[_lib.Context] = None, hkl: Optional[np.ndarray] = None,
+               box=None) -> np.ndarray:
+    """[n_vectors, 4] = (Re A, Im A, |A|², Σ_m |F_m|²): pd_direct at the
+    q-vectors qvec, or, given integer lattice indices hkl and the box sides,
+    pd_direct_lattice at q = 2π·hkl/box (per-point phase tables on the
+    device, the reference's PhaseTable, src/explicit.rs:85-135)."""
     ctx = ctx or _lib.default_context()
     xyz = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
     kind = np.ascontiguousarray(kind, dtype=np.uint32)
     ff = np.ascontiguousarray(ff, dtype=np.float64)
-    qvec = np.ascontiguousarray(qvec, dtype=np.float64).reshape(-1, 3)
+    if hkl is not None:
+        hkl = np.asarray(hkl).reshape(-1, 3)
+        if np.any(np.abs(hkl) > np.iinfo(np.int32).max):
+            raise ValidationError("lattice indices beyond the int32 range")
+        hkl = np.ascontiguousarray(hkl, dtype=np.int32)
+        box = np.ascontiguousarray(box, dtype=np.float64).reshape(3)
+        n_vec = len(hkl)
+    else:
+        qvec = np.ascontiguousarray(qvec, dtype=np.float64).reshape(-1, 3)
+        n_vec = len(qvec)
     w = None if weight is None else np.ascontiguousarray(weight, dtype=np.float64)
     r = _lib.PdDirectRequest()
     r.n_points = len(kind)
@@ -98,12 +111,17 @@ def amplitudes(xyz: np.ndarray, kind: np.ndarray, ff: np.ndarray, qvec: np.ndarr
     r.n_kinds = int(ff.shape[0])
     r.reserved = 0
     r.ff = _lib.dptr(ff)
-    r.n_vectors = len(qvec)
-    r.qvec = _lib.dptr(qvec)
+    r.n_vectors = n_vec
+    r.qvec = _lib.dptr(qvec if hkl is None else None)
     r.n_molecules = int(n_molecules)
     r.weight = _lib.dptr(w)
-    out = np.empty((len(qvec), 4), dtype=np.float64)
-    _lib.check(_lib.lib().pd_direct(ctx.handle, C.byref(r), _lib.dptr(out)), ctx.handle)
+    out = np.empty((n_vec, 4), dtype=np.float64)
+    if hkl is None:
+        _lib.check(_lib.lib().pd_direct(ctx.handle, C.byref(r), _lib.dptr(out)), ctx.handle)
+    else:
+        _lib.check(_lib.lib().pd_direct_lattice(
+            ctx.handle, C.byref(r), hkl.ctypes.data_as(C.POINTER(C.c_int32)), _lib.dptr(box),
+            _lib.dptr(out)), ctx.handle)
     return out
 
 
@@ -174,7 +192,8 @@ class DirectTransform:
         kind = np.searchsorted(used, structure.ids)
         ff = _kind_table(used, self.formfactors, qnorm)
         n = self.num_molecules or 1
-        rows = amplitudes(structure.pos, kind, ff, qvec, n, ctx=self.ctx)
+        rows = amplitudes(structure.pos, kind, ff, None, n, ctx=self.ctx, hkl=self.indices,
+                          box=box_sides)
         if self.grid is not None:
             q, g = self.grid.group(qnorm, rows[:, 2:4])
         else:
@@ -200,7 +219,7 @@ class DirectTransform:
         def amp(xyz, knd, table, weight=None):
             if len(knd) == 0:
                 return np.zeros(len(qvec), dtype=np.complex128)
-            r = amplitudes(xyz, knd, table, qvec, 1, weight, ctx)
+            r = amplitudes(xyz, knd, table, None, 1, weight, ctx, hkl=self.indices, box=box_sides)
             return r[:, 0] + 1j * r[:, 1]
 
         a = amp(structure.pos, kind, _kind_table(used, self.formfactors, qnorm))

@@ -53,6 +53,48 @@ def test_pd_direct_kinds_and_molecule_ends_across_stages(gpu_ctx, n, n_mol, kind
         assert np.max(np.abs(got[:, c] - ref[:, c]) / scale) < 1e-12, c
 
 
+def _rows_close(got, ref, ff, w, n):
+    fmax = (np.abs(ff).max(axis=0) * (np.abs(w).sum() if w is not None else n)) ** 2
+    for c in range(4):
+        scale = fmax if c >= 2 else np.sqrt(fmax)
+        assert np.max(np.abs(got[:, c] - ref[:, c]) / scale) < 1e-12, c
+
+
+@pytest.mark.parametrize("n,n_mol,p_max,weighted,kinds", [
+    (1, 1, 5, False, 3), (1000, 1, 6, False, 3), (2048, 4, 12, True, 3), (4500, 3, 100, False, 3),
+    (3000, 1, 40, True, 20), (6000, 2000, 4, False, 3), (2053, 1, 3, False, 1)])
+def test_pd_direct_lattice_phase_tables_match_oracle(gpu_ctx, n, n_mol, p_max, weighted, kinds):
+    """pd_direct_lattice (per-point phase tables, negative indices by
+    conjugation) against the oracle's rows at q = 2π·hkl/L, on a box that is
+    not cubic, and against pd_direct at the same vectors."""
+    xyz, kind, L = _box(n, n + p_max, kinds=kinds)
+    box = [L, L * 1.1, L * 0.9]
+    hkl = miller_indices(p_max)
+    qv = q_vectors(hkl, box)
+    rng = np.random.default_rng(1)
+    ff = rng.uniform(0.5, 8.0, (kinds, len(qv)))
+    w = rng.uniform(0.0, 2.0, n) if weighted else None
+    got = amplitudes(xyz, kind, ff, None, n_mol, w, gpu_ctx, hkl=hkl, box=box)
+    _rows_close(got, O.direct_rows(xyz, kind, ff, qv, n_mol, w), ff, w, n)
+    _rows_close(got, amplitudes(xyz, kind, ff, qv, n_mol, w, gpu_ctx), ff, w, n)
+
+
+def test_pd_direct_lattice_arbitrary_indices_and_the_sincos_fallback(gpu_ctx):
+    """Unsorted lattice vectors with mixed signs and the zero vector; indices
+    beyond the table bound (600) take the sincos kernel; both match the
+    oracle."""
+    xyz, kind, L = _box(1500, 7, kinds=4)
+    box = [L, L * 1.3, L * 0.7]
+    rng = np.random.default_rng(5)
+    for hmax in (30, 600):
+        hkl = rng.integers(-hmax, hmax + 1, (700, 3))
+        hkl[0] = 0
+        qv = q_vectors(hkl, box)
+        ff = rng.uniform(0.5, 8.0, (4, len(qv)))
+        got = amplitudes(xyz, kind, ff, None, 3, None, gpu_ctx, hkl=hkl, box=box)
+        _rows_close(got, O.direct_rows(xyz, kind, ff, qv, 3), ff, None, len(kind))
+
+
 def test_single_molecule_box_and_two_identical_molecules(gpu_ctx):
     """N = 1: S_eff ≡ 1 and P ≡ total; two well-separated identical dumbbells:
     the per-molecule form factor equals the one-molecule intensity
