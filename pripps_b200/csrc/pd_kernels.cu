@@ -1132,9 +1132,9 @@ __global__ void __launch_bounds__(PD_DIRECT_THREADS)
 // Direct transform at reciprocal-lattice vectors q = 2π·(h, k, l)/L: the phase
 // of a term is e^{i2πh·x/Lx}·e^{i2πk·y/Ly}·e^{i2πl·z/Lz}. Per stage of points
 // the block builds, in shared memory, each point's powers e^{i2πn·x_a/L_a} for
-// n = 0..nmax on every axis (e^{i2π·x_a/L_a} from one sincos, then successive
-// products, negative n by conjugation: the reference's PhaseTable,
-// src/explicit.rs:85-135). A term then costs three table reads and two
+// n = 0..nmax on every axis (segments of a row start from a sincos and step by
+// products with e^{i2π·x_a/L_a}; negative n by conjugation: the reference's
+// PhaseTable, src/explicit.rs:85-135). A term then costs three table reads and two
 // complex products instead of a sincos. Same chunks, partial layout and
 // reduction as pd_direct_chunks; 256 threads own 3 × 256 vectors.
 constexpr int PD_DTAB_THREADS = 256;
@@ -1196,17 +1196,29 @@ __global__ void __launch_bounds__(PD_DTAB_THREADS, 2)
     for (int64_t s0 = p0; s0 < p1; s0 += npts) {
         const int ns = static_cast<int>(min(static_cast<int64_t>(npts), p1 - s0));
         __syncthreads();  // the previous stage's table is read
-        // one thread per (point, axis): the row e^{i2πn·x_a/L_a}, n = 0..stride-1
-        for (int t = tid; t < 3 * ns; t += T) {
-            const int pt = t / 3, a = t - 3 * pt;
+        // the rows e^{i2πn·x_a/L_a}, n = 0..stride-1, one per (point, axis),
+        // each cut into up to 16-entry segments so that every thread takes
+        // part: a segment starts from its own sincos and steps by products
+        const int rows = 3 * ns;
+        const int nseg = max(1, min((stride + 15) / 16, T / rows));
+        const int seglen = (stride + nseg - 1) / nseg;
+        for (int t = tid; t < rows * nseg; t += T) {
+            const int rw = t / nseg, sg = t - rw * nseg;
+            const int pt = rw / 3, a = rw - 3 * pt;
+            const int n0 = sg * seglen, n1 = min(stride, n0 + seglen);
             const double x = xyz[3 * (s0 + pt) + a];
             const double L = a == 0 ? lx : (a == 1 ? ly : lz);
+            const double th = 2.0 * 3.141592653589793 * x / L;
             double sn, cs;
-            sincos(2.0 * 3.141592653589793 * x / L, &sn, &cs);
+            sincos(th, &sn, &cs);
             const double2 step = make_double2(cs, sn);
             double2 e = make_double2(1.0, 0.0);
-            double2 *row = pd_dtab + (3 * pt + a) * stride;
-            for (int n = 0; n < stride; ++n) {
+            if (n0 > 0) {
+                sincos(static_cast<double>(n0) * th, &sn, &cs);
+                e = make_double2(cs, sn);
+            }
+            double2 *row = pd_dtab + rw * stride;
+            for (int n = n0; n < n1; ++n) {
                 row[n] = e;
                 e = cmul(e, step);
             }
