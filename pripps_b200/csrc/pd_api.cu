@@ -551,7 +551,12 @@ constexpr double RR_QUANTUM = 1.0e9;   // work a request adds per round-robin tu
 // Requests of at most this much work (≈1.4 ms alone) skip the steps: at
 // admission their tiles go to an express lane whose stream has the highest
 // priority, so its CTAs take the first SM slots that the running step frees.
-constexpr double EXPRESS_COST = 1.0e10;
+// (1e11 measured worse: 400 requests at once 5.87e12 against 6.81e12
+// pair·q/s, p99 of the 10,000-request stream at 60/s 396 against 312 ms.)
+#ifndef PD_EXPRESS_COST
+#define PD_EXPRESS_COST 1.0e10
+#endif
+constexpr double EXPRESS_COST = PD_EXPRESS_COST;
 constexpr int EXPRESS = STEP_BUFS;  // row of the express lanes
 static_assert((STEP_BUFS + 1) * STEP_LANES <= 32, "lane bits of PdTicket::used_streams");
 
