@@ -1268,10 +1268,10 @@ __global__ void __launch_bounds__(PD_DTAB_THREADS, 2)
 
 // Per q-vector: A = Σ chunks, Σ_m |F_m|² with the slices of a molecule joined
 // first. out[v] = (Re A, Im A, |A|², Σ_m |F_m|²). A block takes 32 vectors (a
-// lane each); its 8 warps sum 8 fixed runs of whole molecules' chunks, each in
+// lane each); its 32 warps sum 32 fixed runs of whole molecules' chunks, each in
 // chunk order, and the run totals are added in run order: the same sums, in
 // the same order, on every call.
-constexpr int PD_DIRECT_RED_WARPS = 8;
+constexpr int PD_DIRECT_RED_WARPS = 32;
 
 __global__ void __launch_bounds__(32 * PD_DIRECT_RED_WARPS)
     pd_direct_reduce(const double *__restrict__ part, int64_t n_vec, int64_t n_chunks,
