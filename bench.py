@@ -103,13 +103,18 @@ class ClockSampler:
                 "power_w_median": statistics.median(power) if power else None}
 
 
-def cpu_sample(w, n_sample=6000, n_q=8, threads=0):
+def cpu_sample(w, n_sample=6000, n_q=0, threads=0):
     """Time the FP64 oracle (the reference's Debye code restated, q-parallel
     on host threads) on a bounded sample of the workload: the first
-    `n_sample` atoms and `n_q` grid points spread over the q range."""
+    `n_sample` atoms and `n_q` grid points spread over the q range (n_q <= 0:
+    two per host core, so that every core has work). Returns (rate, pair·q,
+    seconds, description, threads used)."""
     from oracle import oracle as O
     req = w.request
     n = min(n_sample, req.n_atoms)
+    cores = os.cpu_count() or 1
+    if n_q <= 0:
+        n_q = max(16, 2 * cores)
     qi = np.unique(np.linspace(0, req.nq - 1, n_q).astype(np.int64)).astype(np.uint32)
     xyz = (req.xyz[0] if req.xyz.ndim == 3 else req.xyz)[:n]
     t0 = time.perf_counter()
@@ -132,7 +137,8 @@ def cpu_sample(w, n_sample=6000, n_q=8, threads=0):
                       req.qmin, req.qmax, req.nq, qi, threads)
     dt = time.perf_counter() - t0
     pq = n * (n - 1) // 2 * len(qi)
-    return pq / dt, pq, dt, f"first {n} of {req.n_atoms} atoms × {len(qi)} of {req.nq} q points"
+    return (pq / dt, pq, dt, f"first {n} of {req.n_atoms} atoms × {len(qi)} of {req.nq} q points",
+            min(cores, len(qi)))
 
 
 def run_reference(args, ws, rank):
@@ -148,7 +154,7 @@ def run_reference(args, ws, rank):
     rates, times = [], []
     sample = None
     for _ in range(args.steps):
-        rate, pq, dt, sample = cpu_sample(w, args.cpu_atoms, args.cpu_q)
+        rate, pq, dt, sample, cores = cpu_sample(w, args.cpu_atoms, args.cpu_q)
         rates.append(rate)
         times.append(dt)
     pq_total = pq * len(times)
@@ -345,8 +351,8 @@ def run_ours(args, ws, rank, local):
         fixed_achieved = fixed * kernel_pair_q / (launch_ms * 1e-3) / 1e12
         cpu = None
         if not args.no_cpu and ws == 1:  # the host-core baseline is an N = 1 figure
-            rate, pq, dt, sample = cpu_sample(w, args.cpu_atoms, args.cpu_q)
-            cpu = {"value": rate, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port",
+            rate, pq, dt, sample, used = cpu_sample(w, args.cpu_atoms, args.cpu_q)
+            cpu = {"value": rate, "unit": UNIT, "cores": used, "kind": "port",
                    "sample": sample, "seconds": dt}
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
@@ -546,7 +552,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--fp64-nq", type=int, default=64)
     ap.add_argument("--cpu-atoms", type=int, default=6000)
-    ap.add_argument("--cpu-q", type=int, default=8)
+    ap.add_argument("--cpu-q", type=int, default=0,
+                    help="q points of the CPU baseline sample (0: two per host core)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--serve", action="store_true", help="serving-stream benchmark")
