@@ -39,6 +39,26 @@ UNIT = "pair·q/s"
 # FP32 flops of one pair·q in the class-mode inner loop: recurrence step
 # (FFMA + FADD = 3) + accumulation (FFMA = 2).
 FLOPS_PER_PAIRQ = {"class": 5, "weighted": 7}
+PROFILES = ("atoms", "excluded", "hydration", "atom_excluded", "atom_hydration",
+            "excluded_hydration")
+
+
+def profile_errors(got, ref):
+    """Per-profile max error of [6, m] tables: relative for the three self
+    profiles (>= 0); the cross profiles, which change sign, normalised by
+    sqrt(self_a·self_b) (the Cauchy-Schwarz bound of a cross term). Rows that
+    are zero in both (no solvent) give 0."""
+    err = []
+    pairs = {3: (0, 1), 4: (0, 2), 5: (1, 2)}
+    for r in range(6):
+        d = np.abs(got[r] - ref[r])
+        scale = np.abs(ref[r]) if r < 3 else np.sqrt(np.abs(ref[pairs[r][0]] * ref[pairs[r][1]]))
+        m = scale > 0
+        e = float(np.max(d[m] / scale[m])) if m.any() else 0.0
+        if np.any(d[~m] > 0):
+            e = float("inf")
+        err.append(e)
+    return err
 
 
 def dist_env():
@@ -280,6 +300,7 @@ def run_ours(args, ws, rank, local):
 
     # ---- plain FP64 kernel on the same structure (bounded q grid)
     fp64 = None
+    parity = None
     if rank == 0 and not args.no_fp64:
         r64 = w.with_grid(args.fp64_nq, "fp64")
         p64 = C.c_void_p()
@@ -296,8 +317,42 @@ def run_ours(args, ws, rank, local):
         e1.record(stream)
         torch.cuda.synchronize()
         ms64 = e0.elapsed_time(e1)
-        pq64 = w.pairs * r64.nq
+        pq64 = w.pairs * r64.nq * r64.n_frames
         lib.pd_plan_destroy(ctx.handle, p64)
+        # accuracy of the timed FP32 result against the FP64 kernel: on a
+        # grid whose points are every d-th point of the timed grid (d divides
+        # nq - 1), else on a separate grid solved by both forms
+        steps = [d for d in range(1, req.nq) if (req.nq - 1) % d == 0 and
+                 8 <= (req.nq - 1) // d <= 63]
+        if steps:
+            d = min(steps)
+            rp = w.with_grid((req.nq - 1) // d + 1, "fp64")
+            ours, how = result_dev[:, ::d], f"every {d}th point of the timed grid"
+        else:
+            rp, ours, how = r64, None, f"a {r64.nq}-point grid solved by both forms"
+        pp = C.c_void_p()
+        cp = rp.c_struct()
+        _lib.check(lib.pd_plan_create(ctx.handle, C.byref(cp), C.byref(pp)), ctx.handle)
+        outp = torch.empty((6, rp.nq), dtype=torch.float64, device=f"cuda:{local}")
+        _lib.check(lib.pd_plan_execute(ctx.handle, pp, xyz.data_ptr(), outp.data_ptr(), sp),
+                   ctx.handle)
+        torch.cuda.synchronize()
+        lib.pd_plan_destroy(ctx.handle, pp)
+        ref64 = outp.cpu().numpy()
+        if ours is None:
+            r32 = w.with_grid(r64.nq, args.precision)
+            p32 = C.c_void_p()
+            c32 = r32.c_struct()
+            _lib.check(lib.pd_plan_create(ctx.handle, C.byref(c32), C.byref(p32)), ctx.handle)
+            _lib.check(lib.pd_plan_execute(ctx.handle, p32, xyz.data_ptr(), outp.data_ptr(), sp),
+                       ctx.handle)
+            torch.cuda.synchronize()
+            lib.pd_plan_destroy(ctx.handle, p32)
+            ours = outp.cpu().numpy()
+        parity = {"max_err_vs_fp64_kernel": dict(zip(PROFILES, profile_errors(ours, ref64))),
+                  "q_points": int(rp.nq), "grid": how, "tolerance": 1e-5,
+                  "normalisation": "self profiles relative; cross profiles by "
+                                   "sqrt(self_a·self_b)"}
         fp64 = {"value": pq64 / (ms64 * 1e-3), "unit": UNIT, "nq": r64.nq, "ms": ms64,
                 "fp32_over_fp64": (w.pair_q / (ms_per_step * 1e-3)) / (pq64 / (ms64 * 1e-3))}
 
@@ -385,6 +440,7 @@ def run_ours(args, ws, rank, local):
                                      f"{flops} FLOP per pair·q (species-class factoring, "
                                      "Reinsch form), so the figure exceeds the FP32 peak"}},
             "fp64_kernel": fp64,
+            "parity": parity,
             "cpu_baseline": cpu,
             "clocks": clk,
             "parallelism": f"tile-sharded solve over {ws} GPUs + NCCL all-reduce" if ws > 1

@@ -80,8 +80,9 @@ class Workload:
         r = self.request
         if self.name == "sphere_grid_solvent_10k":
             return grid_solvent_request(self.globule, r.qmin, r.qmax, nq, precision)
+        frames = r.xyz if r.xyz.ndim == 3 else None  # a trajectory keeps its frames
         return globule_request(self.globule, r.qmin, r.qmax, nq, r.ff_excluded is not None,
-                               precision)
+                               precision, frames, r.frame_weights)
 
     @property
     def pairs(self) -> int:
