@@ -141,6 +141,17 @@ def test_workload_requests():
     exp = w.globule.exposed
     assert np.all(r.hyd_weights[~exp] == 0)
     assert np.allclose(r.hyd_weights[exp], wfull[w.globule.elements[exp]])
+    # the same structure on another grid keeps its solvent model
+    g = w.with_grid(64, "fp64")
+    assert g.nq == 64 and g.precision == "fp64" and np.array_equal(g.xyz, r.xyz)
+    assert np.array_equal(g.hyd_weights, r.hyd_weights)
+
+
+def test_trajectory_workload_on_another_grid_keeps_its_frames():
+    w = workloads.trajectory_5k_256(n_frames=6)
+    g = w.with_grid(24, "fp64")
+    assert g.n_frames == 6 and np.array_equal(g.xyz, w.request.xyz)
+    assert np.array_equal(g.frame_weights, w.request.frame_weights)
 
 
 def _tiny_map():
