@@ -3,6 +3,7 @@
 Tests marked `gpu` need an sm_100 device and call the CUDA backend through
 its C ABI; everything else runs on the CPU (oracle, host logic, ABI exports).
 """
+import hashlib
 import json
 import sys
 from pathlib import Path
@@ -23,6 +24,19 @@ def pytest_configure(config):
 
 def load_golden(name):
     return json.loads((GOLDEN / name).read_text())
+
+
+def request_digest(req) -> str:
+    """SHA-256 of a DebyeRequest's inputs (positions, species, form-factor
+    tables, hydration weights, grid): ties an oracle fixture to the exact
+    inputs it was computed from."""
+    h = hashlib.sha256()
+    for a in (req.xyz, np.asarray(req.species).astype(np.uint32), req.ff_atoms,
+              req.ff_excluded, req.hyd_weights, req.ff_water):
+        if a is not None:
+            h.update(np.ascontiguousarray(a, dtype=a.dtype).tobytes())
+    h.update(np.array([req.qmin, req.qmax, req.nq], dtype=np.float64).tobytes())
+    return h.hexdigest()
 
 
 def term_errors(got, ref):

@@ -1,6 +1,9 @@
 """Regenerate foxs_elements.yaml from the reference's FoXS form-factor asset.
 
-    python pripps_b200/data/make_foxs_subset.py /path/to/pripps/assets/foxs_formfactors.yaml
+    python tests/golden/make_foxs_subset.py /path/to/pripps/assets/foxs_formfactors.yaml
+
+Writes pripps_b200/data/foxs_elements.yaml (the form-factor input of the
+synthetic workloads).
 
 Keeps the entries the synthetic workloads use — the C/N/O/S elements (their
 Cromer–Mann Gaussians, radii and displaced volumes) and H2O with the H it is
@@ -55,10 +58,12 @@ def main(src):
         tag, val = spec.get("ff", spec.get("formfactor"))
         parts.append(f"ff: !{tag} {_flow(val)}")
         lines.append(f"{name}: {{ " + ", ".join(parts) + " }")
-    out = Path(__file__).with_name("foxs_elements.yaml")
+    out = Path(__file__).resolve().parents[2] / "pripps_b200" / "data" / "foxs_elements.yaml"
     out.write_text("\n".join(lines) + "\n")
     print(out)
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/assets/foxs_formfactors.yaml")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_foxs_subset.py /path/to/pripps/assets/foxs_formfactors.yaml")
+    main(sys.argv[1])

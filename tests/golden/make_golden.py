@@ -1,6 +1,6 @@
 """Generate the golden fixtures of the parity tests from the reference's test data.
 
-    python tests/golden/make_golden.py [/path/to/pripps]
+    python tests/golden/make_golden.py /path/to/pripps
 
 Reads (never at test time) the reference's lysozyme fixtures and assets:
   tests/lysozyme/4lzt.xyz        129 residue beads
@@ -112,4 +112,6 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py /path/to/pripps (the reference checkout)")
+    main(sys.argv[1])
