@@ -321,6 +321,14 @@ int pd_autotune(pd_ctx *ctx, uint64_t n_atoms, uint64_t nq, uint32_t precision);
 int pd_plan_inspect(pd_ctx *ctx, const pd_request *req, uint64_t *n_classes,
                     uint64_t *n_padded, uint64_t *n_tiles, uint64_t *pairs_covered);
 
+/* Host-only: device bytes one solve of `req` holds with the tuning the
+ * context would pick (ctx may be NULL: default tuning). host_coordinates != 0
+ * counts the device copy of the coordinates that pd_solve and pd_submit make;
+ * 0 is the layout of a plan execution or of pd_solve_noalloc, whose
+ * coordinates are the caller's device memory. No reference counterpart. */
+int pd_request_device_bytes(pd_ctx *ctx, const pd_request *req, int host_coordinates,
+                            uint64_t *device_bytes);
+
 /* Measured FP32 issue peak of the device: FFMA throughput of a register-only
  * microbenchmark, in TFLOP/s at the clock the device runs during the call. */
 int pd_measure_fp32_peak(pd_ctx *ctx, double *tflops_ffma, double *tflops_ffma2);
@@ -346,14 +354,22 @@ uint64_t pd_launch_count(pd_ctx *ctx);
  * [n_frames][N][3]; the [6][nq] result (or the frame-weighted mean) is
  * written to out_terms_dev, DEVICE memory. The work is enqueued on `stream`
  * (a cudaStream_t of the current device; NULL = legacy default stream) and
- * the call returns without waiting for it.
+ * the call returns without waiting for it. It uploads the request's tables
+ * and tile list from host memory that lives only during the call, so it
+ * cannot be captured into a CUDA graph: on a stream that is capturing it
+ * returns PD_EINVAL before any device work. Because it does not wait, a
+ * device-side failure cannot be returned: a bounded wait inside the pair
+ * kernel that expired leaves NaN in the affected rows of out_terms_dev, so
+ * check the result for NaN after synchronising the stream.
  *
  * Limits and sharing:
  *  - A request whose device layout (tables, tile list, packed atoms, tile
  *    partial sums) needs more than PD_NOALLOC_SCRATCH_BYTES fails with
  *    PD_EBUDGET and a message naming both sizes, before any device work.
- *    As a guide, an FP32 solve of 40,000 atoms with solvent at nq = 500 fits;
- *    100,000 atoms at nq = 1,000 needs about 240 MB and is refused.
+ *    pd_request_device_bytes(ctx, req, 0, &bytes) gives a request's need
+ *    beforehand. As a guide, an FP32 solve of 40,000 atoms with solvent at
+ *    nq = 500 fits; 100,000 atoms at nq = 1,000 needs about 240 MB and is
+ *    refused.
  *  - The array occupies PD_NOALLOC_SCRATCH_BYTES of memory on every GPU that
  *    loads the library's device code, until the process exits.
  *  - Every call shares the array, which keeps the previous call's contents;

@@ -122,6 +122,7 @@ SIGNATURES = {
                                 C.c_uint32]),
     "pd_autotune": (C.c_int, [_P, C.c_uint64, C.c_uint64, C.c_uint32]),
     "pd_plan_inspect": (C.c_int, [_P, C.POINTER(PdRequest), _U64P, _U64P, _U64P, _U64P]),
+    "pd_request_device_bytes": (C.c_int, [_P, C.POINTER(PdRequest), C.c_int, _U64P]),
     "pd_measure_fp32_peak": (C.c_int, [_P, _D, _D]),
     "pd_launch_count": (C.c_uint64, [_P]),
     "pd_solve_noalloc": (C.c_int, [C.POINTER(PdRequest), C.c_void_p, C.c_void_p, C.c_void_p]),

@@ -1615,6 +1615,28 @@ int pd_plan_inspect(pd_ctx *ctx, const pd_request *req, uint64_t *n_classes, uin
     return PD_OK;
 }
 
+int pd_request_device_bytes(pd_ctx *ctx, const pd_request *req, int host_coordinates,
+                            uint64_t *device_bytes) {
+    if (!req || !device_bytes) return PD_EINVAL;
+    std::string msg;
+    int rc = pd::validate_request(req, false, msg);
+    if (rc) {
+        if (ctx) ctx->set_error(msg);
+        return rc;
+    }
+    Tuning tun = tuning_for(ctx, static_cast<int64_t>(req->n_atoms), static_cast<int64_t>(req->nq),
+                            static_cast<int>(req->precision),
+                            static_cast<int64_t>(req->n_frames));
+    Plan P;
+    rc = pd::build_plan(req, req->species, req->hyd_weights, tun, P, msg);
+    if (rc) {
+        if (ctx) ctx->set_error(msg);
+        return rc;
+    }
+    *device_bytes = make_layout(P, host_coordinates != 0).total;
+    return PD_OK;
+}
+
 int pd_measure_fp32_peak(pd_ctx *ctx, double *tflops_ffma, double *tflops_ffma2) {
     if (!ctx) return PD_EINVAL;
     cudaSetDevice(ctx->device);
@@ -2138,9 +2160,10 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[PD_NOALLOC_SCRA
 struct NoallocDevice {
     char *scratch = nullptr;      // device address of g_noalloc_scratch
     std::unique_ptr<pd_ctx> ctx;  // launch bookkeeping only: no stream, no pool
+    std::mutex mu;                // one call at a time on this device
 };
-std::mutex g_noalloc_mu;
-std::map<int, NoallocDevice> g_noalloc;  // per device ordinal, set up on first use
+std::mutex g_noalloc_mu;  // guards the map only
+std::map<int, std::unique_ptr<NoallocDevice>> g_noalloc;  // per device ordinal, set up on first use
 
 int noalloc_fail(int rc, const std::string &m) {
     std::lock_guard<std::mutex> g(g_err_mu);
@@ -2200,7 +2223,7 @@ int noalloc_validate(const pd_request *req, std::string &msg) {
 NoallocDevice *noalloc_device(int dev, int *rc) {
     std::lock_guard<std::mutex> g(g_noalloc_mu);
     auto it = g_noalloc.find(dev);
-    if (it != g_noalloc.end()) return &it->second;
+    if (it != g_noalloc.end()) return it->second.get();
     int major = 0, sms = 0;
     cudaError_t e = cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -2219,18 +2242,18 @@ NoallocDevice *noalloc_device(int dev, int *rc) {
                                            cudaGetErrorString(e));
         return nullptr;
     }
-    NoallocDevice nd;
-    nd.scratch = static_cast<char *>(p);
-    nd.ctx = std::make_unique<pd_ctx>();
-    nd.ctx->device = dev;
-    nd.ctx->sm_count = sms;
+    auto nd = std::make_unique<NoallocDevice>();
+    nd->scratch = static_cast<char *>(p);
+    nd->ctx = std::make_unique<pd_ctx>();
+    nd->ctx->device = dev;
+    nd->ctx->sm_count = sms;
     e = pd::prepare_pair_kernels();  // launch attributes, before any capture
     if (e != cudaSuccess) {
         *rc = noalloc_fail(PD_EDEVICE, std::string("pd_solve_noalloc: kernel set-up failed: ") +
                                            cudaGetErrorString(e));
         return nullptr;
     }
-    return &g_noalloc.emplace(dev, std::move(nd)).first->second;
+    return g_noalloc.emplace(dev, std::move(nd)).first->second.get();
 }
 
 }  // namespace
@@ -2257,6 +2280,24 @@ extern "C" int pd_solve_noalloc(const pd_request *req, const double *xyz_dev,
                                 " bytes of device scratch; the fixed scratch holds " +
                                 std::to_string(static_cast<uint64_t>(PD_NOALLOC_SCRATCH_BYTES)) +
                                 " (use pd_solve or a plan for larger requests)");
+    // The plan is uploaded from a host image that lives only for this call,
+    // which a captured graph would replay after it is gone: the first CUDA
+    // call of the entry point refuses a capturing stream.
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        const cudaError_t ce = cudaStreamIsCapturing(st, &cs);
+        if (ce == cudaErrorNoDevice || ce == cudaErrorInsufficientDriver)
+            return noalloc_fail(PD_ENODEV, std::string("pd_solve_noalloc: no CUDA device: ") +
+                                               cudaGetErrorString(ce));
+        if (ce != cudaSuccess || cs != cudaStreamCaptureStatusNone)
+            return noalloc_fail(PD_EINVAL,
+                                std::string("pd_solve_noalloc: the stream is being captured "
+                                            "into a CUDA graph (capture query: ") +
+                                    cudaGetErrorString(ce) +
+                                    "); this call uploads from call-local host memory and "
+                                    "cannot be captured");
+    }
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess)
@@ -2266,9 +2307,8 @@ extern "C" int pd_solve_noalloc(const pd_request *req, const double *xyz_dev,
     if (!nd) return rc;
     // One call at a time per device on the host; the device work of calls on
     // different streams may still overlap, and then they race on the scratch.
-    std::lock_guard<std::mutex> g(g_noalloc_mu);
+    std::lock_guard<std::mutex> g(nd->mu);
     pd_ctx *ctx = nd->ctx.get();
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
     // Host image of the uploaded part in ordinary heap memory: a copy from
     // pageable memory returns once the driver has taken the bytes, so the
     // image may go out of scope when this call returns.
