@@ -54,6 +54,18 @@ extern "C" {
 #define PD_ECANCELED (-7) /* the request was cancelled before it finished */
 #define PD_ENODEV (-8)    /* no sm_100 device at the requested ordinal */
 
+/* ---- request flags ----
+ * PD_FLAG_TEST_EXPIRED_WAIT is a test hook for the failure path of the FP32
+ * pair kernel: the first tile taken by its first CTA waits for a bulk copy
+ * of atoms that is never issued, with a short poll limit, so that the bounded
+ * wait expires with no copy in flight. That CTA then stops, writes NaN to the
+ * slots of every tile it still takes and sets the request's device status;
+ * blocking calls (pd_solve, pd_plan_execute_host, pd_wait, pd_stream_finish)
+ * return PD_ETIMEOUT, calls that leave the result on the device show NaN
+ * rows, and the context stays usable. It has no effect on PD_FP64 requests,
+ * whose kernel stages nothing. */
+#define PD_FLAG_TEST_EXPIRED_WAIT 0x80000000u
+
 /* ---- precision forms ---- */
 #define PD_FP32_FP64RED 0 /* FP32 recurrence sinc, FP32 per-tile sums, FP64 reduction */
 #define PD_FP64 1         /* plain FP64 sinc and accumulation throughout */
@@ -114,7 +126,7 @@ typedef struct pd_request {
     uint64_t nq;                /* >= 1 */
     uint64_t n_frames;          /* 0 or 1: one structure; > 1: trajectory batch */
     const double *frame_weights;/* [n_frames] weights of the mean, or NULL: uniform */
-    uint32_t flags;             /* reserved, must be 0 */
+    uint32_t flags;             /* 0, or PD_FLAG_TEST_EXPIRED_WAIT (tests only) */
     uint32_t n_lattices;        /* 0..8 lattice sets (ABI version 1: must be 0) */
     const pd_lattice *lattices; /* [n_lattices], read only when n_lattices > 0 */
 } pd_request;
@@ -367,9 +379,9 @@ uint64_t pd_launch_count(pd_ctx *ctx);
  *    partial sums) needs more than PD_NOALLOC_SCRATCH_BYTES fails with
  *    PD_EBUDGET and a message naming both sizes, before any device work.
  *    pd_request_device_bytes(ctx, req, 0, &bytes) gives a request's need
- *    beforehand. As a guide, an FP32 solve of 40,000 atoms with solvent at
- *    nq = 500 fits; 100,000 atoms at nq = 1,000 needs about 240 MB and is
- *    refused.
+ *    beforehand. As a guide, an FP32 solve of 100,000 atoms with solvent at
+ *    nq = 1,000 fits (about 45 MB); 200,000 atoms at nq = 1,000 need about
+ *    115 MB and are refused.
  *  - The array occupies PD_NOALLOC_SCRATCH_BYTES of memory on every GPU that
  *    loads the library's device code, until the process exits.
  *  - Every call shares the array, which keeps the previous call's contents;

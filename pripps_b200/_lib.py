@@ -26,6 +26,8 @@ PD_ENOTFOUND = -6
 PD_ECANCELED = -7
 PD_ENODEV = -8
 
+PD_FLAG_TEST_EXPIRED_WAIT = 0x80000000
+
 PD_FP32_FP64RED = 0
 PD_FP64 = 1
 PRECISIONS = {"fp32": PD_FP32_FP64RED, "fp64": PD_FP64}

@@ -54,6 +54,7 @@ struct Layout {
     uint64_t hres;         // host-only: pinned landing area of the [6][nq] result
     uint64_t stage_bytes;  // pinned image size (upload + result area)
     uint64_t centroid, radius, atoms, slots, pairsum, terms, out, counter;
+    uint64_t status;  // int32 device status of the pair kernel, right after out
     uint64_t lat_idx, hist, lat_err;  // lattice sets: coordinates, pair counts, error flag
     uint64_t total;
 };
@@ -87,7 +88,7 @@ Layout make_layout(const Plan &P, bool host_xyz) {
     L.lat_tiles = take(P.lat_tiles.size() * sizeof(PdLatTile));
     L.upload_bytes = o;
     L.hres = o;
-    L.stage_bytes = align_up(o + 6 * nq * 8, 256);
+    L.stage_bytes = align_up(o + 6 * nq * 8 + 8, 256);  // result and status land here
     L.centroid = take(static_cast<uint64_t>(P.n_frames) * 3 * 8);
     L.radius = take(static_cast<uint64_t>(P.n_frames) * 8);
     L.atoms = take(static_cast<uint64_t>(P.n_pad) * P.n_frames *
@@ -95,7 +96,8 @@ Layout make_layout(const Plan &P, bool host_xyz) {
     L.slots = take(static_cast<uint64_t>(P.slots_per_frame) * P.n_frames * P.nv * P.tun.K * 8);
     L.pairsum = take(static_cast<uint64_t>(P.n_frames) * P.nv * P.n_pairs * nq * 8);
     L.terms = take(static_cast<uint64_t>(P.n_frames) * 6 * nq * 8);
-    L.out = take(6 * nq * 8);
+    L.out = take(6 * nq * 8 + 8);
+    L.status = L.out + 6 * nq * 8;
     L.counter = take(sizeof(int) * 4);
     L.lat_idx = take(P.lat.empty() ? 0 : static_cast<uint64_t>(P.n_pad) * sizeof(int4));
     L.hist = take(static_cast<uint64_t>(P.lat_bins) * 8);
@@ -269,6 +271,23 @@ bool lattice_failed(const Plan &P, const double *terms) {
 constexpr const char *kLatticeMsg =
     "a point of a lattice species lies off its lattice (by more than 1e-6 spacing) or outside "
     "its extents";
+constexpr const char *kExpiredMsg =
+    "a bounded wait in the pair kernel expired (a bulk copy of atoms into shared memory did not "
+    "complete); the result is invalid";
+
+// The outcome of a finished solve from the pair kernel's status word and the
+// host result: an expired wait, then a point off its lattice.
+int result_status(pd_ctx *ctx, const Plan &P, int32_t status, const double *terms) {
+    if (status & PD_DEV_WAIT_EXPIRED) {
+        if (ctx) ctx->set_error(kExpiredMsg);
+        return PD_ETIMEOUT;
+    }
+    if (terms && lattice_failed(P, terms)) {
+        if (ctx) ctx->set_error(kLatticeMsg);
+        return PD_EINVAL;
+    }
+    return PD_OK;
+}
 
 // Fill the pinned staging image (tables, layout, tiles, lists, descriptor).
 int stage_plan(pd_ctx *ctx, DevPlan &dp, const pd_request *req) {
@@ -305,6 +324,8 @@ int stage_plan(pd_ctx *ctx, DevPlan &dp, const pd_request *req) {
     rd.qv = dp.dptr<double>(L.qv);
     rd.slots = dp.dptr<double>(L.slots);
     rd.radius = dp.dptr<double>(L.radius);
+    rd.status = dp.dptr<int32_t>(L.status);
+    rd.flags = P.test_expire ? PD_REQF_TEST_EXPIRE : 0;
     rd.qmin = P.qmin;
     rd.dq = P.dq;
     rd.n_pad = P.n_pad;
@@ -374,6 +395,7 @@ int plan_device(pd_ctx *ctx, const pd_request *req, DevPlan &dp, cudaStream_t st
     }
     stage_plan(ctx, dp, req);
     e = cudaMemcpyAsync(dp.base, dp.stage, dp.L.upload_bytes, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(dp.base + dp.L.status, 0, 8, st);
     if (e != cudaSuccess) {
         free_devplan(ctx, dp, st);
         return cuda_fail(ctx, e, "plan upload");
@@ -469,6 +491,8 @@ int run_devplan(pd_ctx *ctx, DevPlan &dp, double *out_dev, cudaStream_t st,
     const Layout &L = dp.L;
     int rc = pack_devplan(ctx, dp, st);
     if (rc) return rc;
+    // a streamed trajectory keeps the status of all its batches
+    if (!dp.frame_sum) PD_CUDA(ctx, cudaMemsetAsync(dp.base + L.status, 0, 8, st));
     if (ev) cudaEventRecord(ev->first, st);
     if (dp.world > 1)  // the lists also name the other ranks' slots
         PD_CUDA(ctx, cudaMemsetAsync(dp.dptr<double>(L.slots), 0,
@@ -941,9 +965,10 @@ void worker_main(pd_ctx *ctx) {
                     fail(t, PD_EDEVICE, "reduction launch failed");
                     continue;
                 }
+                // the result and the pair kernel's status word behind it
                 cudaMemcpyAsync(t->dp.hptr<double>(t->dp.L.hres), t->dp.dptr<double>(t->dp.L.out),
-                                static_cast<size_t>(6) * t->dp.P.nq * 8, cudaMemcpyDeviceToHost,
-                                sf);
+                                static_cast<size_t>(6) * t->dp.P.nq * 8 + 8,
+                                cudaMemcpyDeviceToHost, sf);
             }
             if (cudaEventCreateWithFlags(&t->done_ev, cudaEventDisableTiming) != cudaSuccess ||
                 cudaEventRecord(t->done_ev, sf) != cudaSuccess) {
@@ -964,16 +989,20 @@ void worker_main(pd_ctx *ctx) {
                 if (q == cudaSuccess) {
                     cudaEventDestroy(t->done_ev);
                     t->done_ev = nullptr;
-                    bool bad_lattice = false;
+                    int rs = PD_OK;
                     if (!t->drained_only) {
                         const double *res = t->dp.hptr<double>(t->dp.L.hres);
-                        t->result.assign(res, res + static_cast<size_t>(6) * t->dp.P.nq);
-                        bad_lattice = lattice_failed(t->dp.P, res);
+                        const size_t n6 = static_cast<size_t>(6) * t->dp.P.nq;
+                        t->result.assign(res, res + n6);
+                        int32_t dev_status = 0;
+                        std::memcpy(&dev_status, res + n6, sizeof(int32_t));
+                        rs = result_status(nullptr, t->dp.P, dev_status, res);
                     }
                     free_devplan(ctx, t->dp, sa);
                     std::lock_guard<std::mutex> lk(ctx->qmu);
-                    t->status = t->drained_only ? PD_ECANCELED : (bad_lattice ? PD_EINVAL : 0);
-                    if (bad_lattice) t->err = kLatticeMsg;
+                    t->status = t->drained_only ? PD_ECANCELED : rs;
+                    if (rs == PD_ETIMEOUT) t->err = kExpiredMsg;
+                    if (rs == PD_EINVAL) t->err = kLatticeMsg;
                     t->t_done = now_s();
                     ctx->done_cv.notify_all();
                     remove = true;
@@ -1137,15 +1166,16 @@ int pd_solve(pd_ctx *ctx, const pd_request *req, double *out_terms) {
     if (rc) return rc;
     rc = run_devplan(ctx, dp, nullptr, ctx->stream);
     if (rc == PD_OK) {
+        int32_t dev_status = 0;
         cudaError_t e = cudaMemcpyAsync(out_terms, dp.dptr<double>(dp.L.out),
                                         static_cast<size_t>(6) * dp.P.nq * 8,
                                         cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(&dev_status, dp.base + dp.L.status, sizeof(int32_t),
+                                cudaMemcpyDeviceToHost, ctx->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
         if (e != cudaSuccess) rc = cuda_fail(ctx, e, "pd_solve");
-        if (rc == PD_OK && lattice_failed(dp.P, out_terms)) {
-            ctx->set_error(kLatticeMsg);
-            rc = PD_EINVAL;
-        }
+        if (rc == PD_OK) rc = result_status(ctx, dp.P, dev_status, out_terms);
     }
     free_devplan(ctx, dp, ctx->stream);
     cudaStreamSynchronize(ctx->stream);
@@ -1248,15 +1278,16 @@ int pd_plan_execute_host(pd_ctx *ctx, pd_plan *plan, const double *xyz_host, dou
     plan->dp.xyz_dev = xyz_dev;
     int rc = run_devplan(ctx, plan->dp, nullptr, ctx->stream);
     if (rc == PD_OK) {
+        int32_t dev_status = 0;
         cudaError_t e = cudaMemcpyAsync(out_terms, plan->dp.dptr<double>(plan->dp.L.out),
                                         static_cast<size_t>(6) * P.nq * 8,
                                         cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(&dev_status, plan->dp.base + plan->dp.L.status, sizeof(int32_t),
+                                cudaMemcpyDeviceToHost, ctx->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
         if (e != cudaSuccess) rc = cuda_fail(ctx, e, "pd_plan_execute_host");
-        if (rc == PD_OK && lattice_failed(P, out_terms)) {
-            ctx->set_error(kLatticeMsg);
-            rc = PD_EINVAL;
-        }
+        if (rc == PD_OK) rc = result_status(ctx, P, dev_status, out_terms);
     }
     cudaFreeAsync(xyz_dev, ctx->stream);
     cudaStreamSynchronize(ctx->stream);
@@ -2115,9 +2146,14 @@ extern "C" int pd_stream_finish(pd_ctx *ctx, pd_stream *s, double *out_terms) {
         const size_t n6 = 6ull * s->dp.P.nq;
         std::vector<double> acc(n6);
         if (rc == PD_OK && !s->failed) {
+            int32_t dev_status = 0;  // of every batch: a stream's plan keeps it
             cudaError_t e = cudaMemcpyAsync(acc.data(), s->d_acc, n6 * 8, cudaMemcpyDeviceToHost, s->cs);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(&dev_status, s->dp.base + s->dp.L.status, sizeof(int32_t),
+                                    cudaMemcpyDeviceToHost, s->cs);
             if (e == cudaSuccess) e = cudaStreamSynchronize(s->cs);
             if (e != cudaSuccess) rc = cuda_fail(ctx, e, "pd_stream_finish");
+            if (rc == PD_OK) rc = result_status(ctx, s->dp.P, dev_status, nullptr);
         } else if (rc == PD_OK) {
             ctx->set_error("the stream failed earlier");
             rc = PD_EDEVICE;
@@ -2320,7 +2356,7 @@ extern "C" int pd_solve_noalloc(const pd_request *req, const double *xyz_dev,
     e = cudaMemcpyAsync(dp.base, image.data(), dp.L.upload_bytes, cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) {
         dp.xyz_dev = xyz_dev;
-        rc = run_devplan(ctx, dp, out_terms_dev, st);  // also zeroes the tile counter
+        rc = run_devplan(ctx, dp, out_terms_dev, st);  // also zeroes the counter and status
     } else {
         rc = cuda_fail(ctx, e, "pd_solve_noalloc: upload");
     }

@@ -12,8 +12,10 @@
 //   * a tile ("job") is (frame, i-block of PD_IBLOCK atoms, contiguous j range
 //     of real atoms of ONE class, q-block of K grid points); it covers the
 //     pairs (i, j) with j > i;
-//   * each of the PD_WARPS warps of a tile writes its warp-reduced partial
-//     sums for the K q-points to its own FP64 slot; a second kernel adds the
+//   * the PD_WARPS warps of a tile keep their warp-reduced FP64 partial sums
+//     for the K q-points in shared memory; at the end of the tile the warps of
+//     one atom class are added in warp order and written to one FP64 slot per
+//     distinct class of the i-block (usually one); a second kernel adds the
 //     slots of every (class pair, q) in a fixed order, so the result does not
 //     depend on which SM ran which tile.
 #pragma once
@@ -45,9 +47,21 @@ struct PdJob {
     int32_t i0;     // first padded i index (multiple of PD_IBLOCK)
     int32_t j0, j1; // padded j range [j0, j1): real atoms of one class
     int32_t qb;     // q-block index
-    int64_t slot;   // first of the PD_WARPS output slots of this tile
+    // bits 0..47: first output slot of this tile; bits 48..55: the slot of
+    // each warp relative to it, 2 bits per warp (warp w at bits 48 + 2w).
+    // Warps of one class share a slot; slot numbers follow the first warp
+    // of each class, so warp 0 always has relative slot 0.
+    int64_t slot;
 };
 static_assert(sizeof(PdJob) == 32, "PdJob layout");
+constexpr int PD_SLOT_MAP_SHIFT = 48;
+constexpr int64_t PD_SLOT_MASK = (int64_t{1} << PD_SLOT_MAP_SHIFT) - 1;
+
+// Bits of the per-request device status word (PdReqDev::status).
+constexpr int32_t PD_DEV_WAIT_EXPIRED = 1;  // a bounded wait for a bulk copy gave up
+
+// PdReqDev::flags
+constexpr int32_t PD_REQF_TEST_EXPIRE = 1;  // test hook: CTA 0 skips its first copy
 
 // Per-request descriptor read by the pair kernels.
 struct PdReqDev {
@@ -57,11 +71,14 @@ struct PdReqDev {
     const double *qv;         // [nq] grid (FP64 form reads it directly)
     double *slots;            // [n_slots][nv][K]
     const double *radius;     // [n_frames] largest atom distance from the centroid
+    int32_t *status;          // PD_DEV_* bits, OR-ed in by the pair kernel
     double qmin, dq;          // grid origin and step
     int32_t n_pad;
     int32_t nq;
     int32_t K;
     int32_t mode;
+    int32_t flags;            // PD_REQF_* bits
+    int32_t pad_;
 };
 
 // Per-class constants for the combine kernel.

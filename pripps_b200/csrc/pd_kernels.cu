@@ -9,12 +9,15 @@
 // u_{k+1} = 2cos(x')·u_k − u_{k−1}, evaluated in Reinsch's difference form
 //   d_{k+1} = d_k − α·u_k,  u_{k+1} = u_k + d_{k+1},  α = 4 sin²(x'/2),
 // which stays accurate for small x' (Reinsch's modification of the Goertzel
-// recurrence; errors grow linearly in k). It is reseeded every K steps from an
-// accurate sincosf(θ). One step plus the accumulation acc_k += σ^k u_k / r is
-// FFMA + FADD + FFMA, all on the FP32 pipes. acc_k sums sin(q_k r)/r over the
-// thread's pairs; dividing by q_k in FP64 afterwards gives Σ sinc(q_k r).
-// Per-tile sums stay in FP32 registers; they are warp-reduced and written as
-// FP64 slots, and every later sum is FP64.
+// recurrence; errors grow linearly in k). It is reseeded every K steps from
+// sin θ and cos θ evaluated in FP32 with a double-float phase and our own
+// fitted polynomials (see sincos_poly). One step plus the accumulation
+// acc_k += σ^k u_k / r is FFMA + FADD + FFMA, all on the FP32 pipes. acc_k
+// sums sin(q_k r)/r over the thread's pairs; dividing by q_k in FP64
+// afterwards gives Σ sinc(q_k r).
+// Per-sub-chunk sums stay in FP32 registers; they are warp-reduced into FP64
+// partial sums in shared memory, merged per atom class at the end of the
+// tile into FP64 slots, and every later sum is FP64.
 //
 // K2 (pd_pairs_fp64): the same tiling with sin(q_k r) from the FP64 sin() for
 // every pair and q, and FP64 accumulation throughout.
@@ -189,8 +192,10 @@ __host__ __device__ __forceinline__ bool residual_q(double q, double radius) {
 // ------------------------------------------------- shared-memory staging (TMA)
 // One-dimensional bulk copies (cp.async.bulk, no multicast) of j-atom chunks
 // into shared memory, completed on an mbarrier. Every wait is bounded: a
-// copy that does not land within ~2^22 polls makes the wait return false and
-// the caller poisons its results with NaN instead of hanging the GPU.
+// copy that does not land within its poll limit makes the wait return false;
+// the pair kernel then stops issuing copies, waits (bounded) for the ones in
+// flight, poisons its results with NaN and sets a status bit the host reads,
+// instead of hanging the GPU.
 __device__ __forceinline__ uint32_t smem_addr(const void *p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
@@ -216,8 +221,8 @@ __device__ __forceinline__ void bulk_copy_to_shared(void *dst, const void *src, 
         "l"(src), "r"(bytes), "r"(smem_addr(bar))
         : "memory");
 }
-__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, uint32_t phase) {
-    for (int it = 0; it < (1 << 22); ++it) {
+__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, uint32_t phase, int polls) {
+    for (int it = 0; it < polls; ++it) {
         uint32_t done;
         asm volatile(
             "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
@@ -409,16 +414,49 @@ constexpr int fp32_min_blocks(int K, int MODE, int NP) {
                                  : (K <= 32 ? 4 : 2);
 }
 
+// Polls of a bulk-copy wait before it gives up: the normal limit, and the
+// short one of the test hook (PD_REQF_TEST_EXPIRE), whose copy is never
+// issued.
+constexpr int PD_WAIT_POLLS = 1 << 22;
+constexpr int PD_TEST_WAIT_POLLS = 1 << 10;
+
+// End of a tile: the warps' FP64 partial sums (part[w·nvk + e], e < nvk) of
+// one class are added in warp order and written to that class's slot; a CTA
+// whose copy wait expired writes NaN instead, and an empty tile zeros.
+__device__ __forceinline__ void merge_tile_slots(const double *__restrict__ part, int nvk,
+                                                 int64_t slot_word, double *__restrict__ slots,
+                                                 bool dead, bool empty) {
+    const int64_t slot0 = slot_word & PD_SLOT_MASK;
+    const int smap = static_cast<int>(slot_word >> PD_SLOT_MAP_SHIFT) & 0xff;
+    const double nan = __longlong_as_double(0x7ff8000000000000ll);
+    for (int e = threadIdx.x; e < nvk; e += blockDim.x) {
+        double a[PD_WARPS];
+        int used = 0;
+#pragma unroll
+        for (int w = 0; w < PD_WARPS; ++w) {
+            const int s = (smap >> (2 * w)) & 3;
+            const double v = part[w * nvk + e];
+            a[s] = (used & (1 << s)) ? a[s] + v : v;
+            used |= 1 << s;
+        }
+#pragma unroll
+        for (int s = 0; s < PD_WARPS; ++s)
+            if (used & (1 << s))
+                slots[(slot0 + s) * nvk + e] = dead ? nan : (empty ? 0.0 : a[s]);
+    }
+}
+
 template <int K, int MODE, int NP>
 __global__ void __launch_bounds__(PD_THREADS, fp32_min_blocks(K, MODE, NP))
-    pd_pairs_fp32(const PdJob *__restrict__ jobs,
-                                                            const int *__restrict__ n_jobs_ptr,
-                                                            const PdReqDev *__restrict__ reqs,
-                                                            int *__restrict__ counter) {
+    pd_pairs_fp32(const PdJob *__restrict__ jobs, const int *__restrict__ n_jobs_ptr,
+                  const PdReqDev *__restrict__ reqs, int *__restrict__ counter) {
     constexpr int NACC = (MODE == PD_MODE_WEIGHTED) ? 2 : 1;
+    constexpr int NV = (MODE == PD_MODE_WEIGHTED) ? 4 : 1;  // FP64 values per q in a slot
     constexpr bool PACKED = (MODE == PD_MODE_CLASS);
     __shared__ int s_job;
     __shared__ __align__(16) float s_qres[K];
+    // per-warp FP64 partial sums of the current tile, [warp][NV][K]
+    __shared__ double s_part[PD_WARPS * NV * K];
     // j atoms of the current and the next stage, staged by bulk copies
     // (PD_FP32_DYN_SMEM bytes of dynamic shared memory)
     extern __shared__ __align__(128) float4 pd_dyn_atoms[];
@@ -434,6 +472,13 @@ __global__ void __launch_bounds__(PD_THREADS, fp32_min_blocks(K, MODE, NP))
     }
     __syncthreads();
     uint32_t phase = 0;  // bit b: parity of buffer b's next completion
+    // Once a copy wait of this CTA expires the CTA is "dead" for the rest of
+    // the launch: it issues no more copies, computes nothing, writes NaN to
+    // the slots of every tile it still takes and flags each tile's request
+    // in its status word. (Uniform across the CTA.)
+    bool dead = false;
+    bool first_tile = true;
+    double *part = s_part + warp * NV * K;
     for (;;) {
         if (threadIdx.x == 0) s_job = atomicAdd(counter, 1);
         __syncthreads();
@@ -471,138 +516,142 @@ __global__ void __launch_bounds__(PD_THREADS, fp32_min_blocks(K, MODE, NP))
         // Every pair distance is at most 2·radius (positions are centred):
         // below π/4 for the step angle Δq·r the seeds skip its reduction.
         const bool general_step = rq.dq * (2.0 * radius) > 0.78;
-
-        if constexpr (PACKED) {
-            const float2 *q2 = reinterpret_cast<const float2 *>(s_qres);
-            // 16-point chunks of this block that lie on the grid. The
-            // small-q residual blocks (the first of a grid) run whole: a
-            // tail check there costs the register spills it saves in steps.
-            const int nchunk = (min(K, rq.nq - kq0) + 15) >> 4;
-            double *slot = rq.slots + (jb.slot + warp) * static_cast<int64_t>(K);
-            const int nstage = (jb.j1 - jb.j0 + PD_JSTAGE - 1) / PD_JSTAGE;
-            if (threadIdx.x == 0 && nstage > 0)
-                bulk_copy_to_shared(s_atoms[0], at + jb.j0,
-                                    static_cast<uint32_t>(min(jb.j1 - jb.j0, PD_JSTAGE)) * 16,
-                                    &s_bar[0]);
-            for (int stg = 0; stg < nstage; ++stg) {
-              const int jss = jb.j0 + stg * PD_JSTAGE;
-              const int jse = min(jb.j1, jss + PD_JSTAGE);
-              if (threadIdx.x == 0 && stg + 1 < nstage)  // its buffer was released at stg - 1
-                  bulk_copy_to_shared(s_atoms[(stg + 1) & 1], at + jse,
-                                      static_cast<uint32_t>(min(jb.j1 - jse, PD_JSTAGE)) * 16,
-                                      &s_bar[(stg + 1) & 1]);
-              const int b = stg & 1;
-              const bool landed = mbar_wait(&s_bar[b], (phase >> b) & 1u);
-              phase ^= 1u << b;
-              const float4 *chunk = s_atoms[b];
-              for (int js = jss; js < jse; js += PD_JFLUSH) {
-                const int je = min(jse, js + PD_JFLUSH);
-                float2 acc[K / 2];
+        const int nstage = dead ? 0 : (jb.j1 - jb.j0 + PD_JSTAGE - 1) / PD_JSTAGE;
+        // test hook: the first tile of CTA 0 waits for a copy that is never
+        // issued, briefly, so that its wait expires with no copy in flight
+        const bool test_skip =
+            (rq.flags & PD_REQF_TEST_EXPIRE) != 0 && blockIdx.x == 0 && first_tile;
+        first_tile = false;
+        const int polls = test_skip ? PD_TEST_WAIT_POLLS : PD_WAIT_POLLS;
+        // thread 0: buffers with a copy in flight, and the parity of each
+        uint32_t inflight = 0, par = 0;
+        auto issue = [&](int b, int j_from, int j_to) {
+            bulk_copy_to_shared(s_atoms[b], at + j_from, static_cast<uint32_t>(j_to - j_from) * 16,
+                                &s_bar[b]);
+            inflight |= 1u << b;
+            par = (par & ~(1u << b)) | (phase & (1u << b));
+        };
+        if (threadIdx.x == 0 && nstage > 0 && !test_skip)
+            issue(0, jb.j0, min(jb.j1, jb.j0 + PD_JSTAGE));
+        for (int stg = 0; stg < nstage; ++stg) {
+            const int jss = jb.j0 + stg * PD_JSTAGE;
+            const int jse = min(jb.j1, jss + PD_JSTAGE);
+            if (threadIdx.x == 0 && stg + 1 < nstage)  // its buffer was released at stg - 1
+                issue((stg + 1) & 1, jse, min(jb.j1, jse + PD_JSTAGE));
+            const int b = stg & 1;
+            const bool got = mbar_wait(&s_bar[b], (phase >> b) & 1u, polls);
+            phase ^= 1u << b;
+            if (threadIdx.x == 0 && got) inflight &= ~(1u << b);
+            // the compute below has warp collectives: decide per warp
+            const bool landed = __all_sync(0xffffffffu, got);
+            const float4 *chunk = s_atoms[b];
+            if (landed) {
+                for (int js = jss; js < jse; js += PD_JFLUSH) {
+                    const int je = min(jse, js + PD_JFLUSH);
+                    const bool first = js == jb.j0;
+                    if constexpr (PACKED) {
+                        const float2 *q2 = reinterpret_cast<const float2 *>(s_qres);
+                        // 16-point chunks of this block that lie on the grid.
+                        // The small-q residual blocks (the first of a grid)
+                        // run whole: a tail check there costs the register
+                        // spills it saves in steps.
+                        const int nchunk = (min(K, rq.nq - kq0) + 15) >> 4;
+                        float2 acc[K / 2];
 #pragma unroll
-                for (int t = 0; t < K / 2; ++t) acc[t] = make_float2(0.0f, 0.0f);
-                if (resid) {
-                    if (general_step)
-                        pairs_range_x2<K, NP, true, true>(chunk, jss, pi, i, ivalid, js, je, qs_hi,
-                                                          qs_lo, dq_hi, dq_lo, q2, acc, K / 16,
-                                                          rchunk);
-                    else
-                        pairs_range_x2<K, NP, true, false>(chunk, jss, pi, i, ivalid, js, je, qs_hi,
-                                                           qs_lo, dq_hi, dq_lo, q2, acc, K / 16,
-                                                           rchunk);
-                } else {
-                    if (general_step)
-                        pairs_range_x2<K, NP, false, true>(chunk, jss, pi, i, ivalid, js, je, qs_hi,
-                                                           qs_lo, dq_hi, dq_lo, q2, acc, nchunk);
-                    else
-                        pairs_range_x2<K, NP, false, false>(chunk, jss, pi, i, ivalid, js, je, qs_hi,
-                                                            qs_lo, dq_hi, dq_lo, q2, acc, nchunk);
-                }
-                // Warp-reduce and add into this warp's slot: K FP64 values,
-                // in sub-chunk order (one warp owns the slot: deterministic).
-                // A chunk that never landed poisons the slot with NaN.
-                const bool first = js == jb.j0;
-                const double bad = __any_sync(0xffffffffu, !landed)
-                                       ? __longlong_as_double(0x7ff8000000000000ll)
-                                       : 0.0;
+                        for (int t = 0; t < K / 2; ++t) acc[t] = make_float2(0.0f, 0.0f);
+                        if (resid) {
+                            if (general_step)
+                                pairs_range_x2<K, NP, true, true>(chunk, jss, pi, i, ivalid, js, je,
+                                                                  qs_hi, qs_lo, dq_hi, dq_lo, q2,
+                                                                  acc, K / 16, rchunk);
+                            else
+                                pairs_range_x2<K, NP, true, false>(chunk, jss, pi, i, ivalid, js,
+                                                                   je, qs_hi, qs_lo, dq_hi, dq_lo,
+                                                                   q2, acc, K / 16, rchunk);
+                        } else {
+                            if (general_step)
+                                pairs_range_x2<K, NP, false, true>(chunk, jss, pi, i, ivalid, js,
+                                                                   je, qs_hi, qs_lo, dq_hi, dq_lo,
+                                                                   q2, acc, nchunk);
+                            else
+                                pairs_range_x2<K, NP, false, false>(chunk, jss, pi, i, ivalid, js,
+                                                                    je, qs_hi, qs_lo, dq_hi, dq_lo,
+                                                                    q2, acc, nchunk);
+                        }
+                        // Warp-reduce and add into this warp's partial sums,
+                        // in sub-chunk order (one warp owns them).
 #pragma unroll
-                for (int t = 0; t < K / 2; ++t) {
-                    const float v0 = warp_sum(acc[t].x);
-                    const float v1 = warp_sum(acc[t].y);
-                    if (lane == ((2 * t) & 31))
-                        slot[2 * t] = (first ? 0.0 : slot[2 * t]) + static_cast<double>(v0) + bad;
-                    if (lane == ((2 * t + 1) & 31))
-                        slot[2 * t + 1] =
-                            (first ? 0.0 : slot[2 * t + 1]) + static_cast<double>(v1) + bad;
-                }
-              }
-              __syncthreads();  // every read of buffer b done before it is refilled
-            }
-        } else {
-            double *slot = rq.slots + (jb.slot + warp) * static_cast<int64_t>(K) * 4;
-            const float wi = ivalid ? pi.w : 0.0f;
-            const int nstage = (jb.j1 - jb.j0 + PD_JSTAGE - 1) / PD_JSTAGE;
-            if (threadIdx.x == 0 && nstage > 0)
-                bulk_copy_to_shared(s_atoms[0], at + jb.j0,
-                                    static_cast<uint32_t>(min(jb.j1 - jb.j0, PD_JSTAGE)) * 16,
-                                    &s_bar[0]);
-            for (int stg = 0; stg < nstage; ++stg) {
-              const int jss = jb.j0 + stg * PD_JSTAGE;
-              const int jse = min(jb.j1, jss + PD_JSTAGE);
-              if (threadIdx.x == 0 && stg + 1 < nstage)  // its buffer was released at stg - 1
-                  bulk_copy_to_shared(s_atoms[(stg + 1) & 1], at + jse,
-                                      static_cast<uint32_t>(min(jb.j1 - jse, PD_JSTAGE)) * 16,
-                                      &s_bar[(stg + 1) & 1]);
-              const int b = stg & 1;
-              const bool landed = mbar_wait(&s_bar[b], (phase >> b) & 1u);
-              phase ^= 1u << b;
-              const float4 *chunk = s_atoms[b];
-              for (int js = jss; js < jse; js += PD_JFLUSH) {
-                const int je = min(jse, js + PD_JFLUSH);
-                float acc[NACC][K];
+                        for (int t = 0; t < K / 2; ++t) {
+                            const float v0 = warp_sum(acc[t].x);
+                            const float v1 = warp_sum(acc[t].y);
+                            if (lane == ((2 * t) & 31))
+                                part[2 * t] = (first ? 0.0 : part[2 * t]) + static_cast<double>(v0);
+                            if (lane == ((2 * t + 1) & 31))
+                                part[2 * t + 1] =
+                                    (first ? 0.0 : part[2 * t + 1]) + static_cast<double>(v1);
+                        }
+                    } else {
+                        const float wi = ivalid ? pi.w : 0.0f;
+                        float acc[NACC][K];
 #pragma unroll
-                for (int a = 0; a < NACC; ++a)
+                        for (int a = 0; a < NACC; ++a)
 #pragma unroll
-                    for (int k = 0; k < K; ++k) acc[a][k] = 0.0f;
-                if (resid) {
-                    if (general_step)
-                        pairs_range<K, MODE, NP, true, true>(chunk, jss, pi, i, ivalid, js, je, qs_hi,
-                                                             qs_lo, dq_hi, dq_lo, s_qres, acc);
-                    else
-                        pairs_range<K, MODE, NP, true, false>(chunk, jss, pi, i, ivalid, js, je, qs_hi,
-                                                              qs_lo, dq_hi, dq_lo, s_qres, acc);
-                } else {
-                    if (general_step)
-                        pairs_range<K, MODE, NP, false, true>(chunk, jss, pi, i, ivalid, js, je, qs_hi,
-                                                              qs_lo, dq_hi, dq_lo, s_qres, acc);
-                    else
-                        pairs_range<K, MODE, NP, false, false>(chunk, jss, pi, i, ivalid, js, je, qs_hi,
-                                                               qs_lo, dq_hi, dq_lo, s_qres, acc);
-                }
-                // Warp-reduce and add into this warp's slot: [4][K] FP64 values.
-                const bool first = js == jb.j0;
-                const double bad = __any_sync(0xffffffffu, !landed)
-                                       ? __longlong_as_double(0x7ff8000000000000ll)
-                                       : 0.0;
+                            for (int k = 0; k < K; ++k) acc[a][k] = 0.0f;
+                        if (resid) {
+                            if (general_step)
+                                pairs_range<K, MODE, NP, true, true>(chunk, jss, pi, i, ivalid, js,
+                                                                     je, qs_hi, qs_lo, dq_hi,
+                                                                     dq_lo, s_qres, acc);
+                            else
+                                pairs_range<K, MODE, NP, true, false>(chunk, jss, pi, i, ivalid, js,
+                                                                      je, qs_hi, qs_lo, dq_hi,
+                                                                      dq_lo, s_qres, acc);
+                        } else {
+                            if (general_step)
+                                pairs_range<K, MODE, NP, false, true>(chunk, jss, pi, i, ivalid, js,
+                                                                      je, qs_hi, qs_lo, dq_hi,
+                                                                      dq_lo, s_qres, acc);
+                            else
+                                pairs_range<K, MODE, NP, false, false>(chunk, jss, pi, i, ivalid,
+                                                                       js, je, qs_hi, qs_lo, dq_hi,
+                                                                       dq_lo, s_qres, acc);
+                        }
+                        // Warp-reduce into this warp's [4][K] partial sums.
 #pragma unroll
-                for (int k = 0; k < K; ++k) {
-                    const float t0 = warp_sum(acc[0][k]);
-                    const float ti = warp_sum(wi * acc[0][k]);
-                    const float tj = warp_sum(acc[NACC - 1][k]);
-                    const float tij = warp_sum(wi * acc[NACC - 1][k]);
-                    if (lane == (k & 31)) {
-                        slot[k] = (first ? 0.0 : slot[k]) + static_cast<double>(t0) + bad;
-                        slot[K + k] = (first ? 0.0 : slot[K + k]) + static_cast<double>(ti) + bad;
-                        slot[2 * K + k] =
-                            (first ? 0.0 : slot[2 * K + k]) + static_cast<double>(tj) + bad;
-                        slot[3 * K + k] =
-                            (first ? 0.0 : slot[3 * K + k]) + static_cast<double>(tij) + bad;
+                        for (int k = 0; k < K; ++k) {
+                            const float t0 = warp_sum(acc[0][k]);
+                            const float ti = warp_sum(wi * acc[0][k]);
+                            const float tj = warp_sum(acc[NACC - 1][k]);
+                            const float tij = warp_sum(wi * acc[NACC - 1][k]);
+                            if (lane == (k & 31)) {
+                                part[k] = (first ? 0.0 : part[k]) + static_cast<double>(t0);
+                                part[K + k] = (first ? 0.0 : part[K + k]) + static_cast<double>(ti);
+                                part[2 * K + k] =
+                                    (first ? 0.0 : part[2 * K + k]) + static_cast<double>(tj);
+                                part[3 * K + k] =
+                                    (first ? 0.0 : part[3 * K + k]) + static_cast<double>(tij);
+                            }
+                        }
                     }
                 }
-              }
-              __syncthreads();  // every read of buffer b done before it is refilled
+            }
+            // every read of buffer b done before it is refilled; an expired
+            // wait in any warp makes the whole CTA dead
+            if (__syncthreads_or(!landed)) {
+                dead = true;
+                break;
             }
         }
-        __syncthreads();  // s_qres and s_job are rewritten by the next tile
+        if (dead && threadIdx.x == 0) {
+            // no copy of this CTA may land in shared memory after it moves
+            // on: wait (bounded) for the ones still in flight
+            for (int b = 0; b < 2; ++b)
+                if (inflight & (1u << b)) mbar_wait(&s_bar[b], (par >> b) & 1u, PD_WAIT_POLLS);
+            atomicOr(rq.status, PD_DEV_WAIT_EXPIRED);
+        }
+        __syncthreads();  // every warp's partial sums are complete
+        merge_tile_slots(s_part, NV * K, jb.slot, rq.slots, dead, nstage == 0 && !dead);
+        __syncthreads();  // s_qres, s_part and s_job are rewritten by the next tile
     }
 }
 
@@ -613,11 +662,14 @@ __global__ void __launch_bounds__(PD_THREADS) pd_pairs_fp64(const PdJob *__restr
                                                             const PdReqDev *__restrict__ reqs,
                                                             int *__restrict__ counter) {
     constexpr int NACC = (MODE == PD_MODE_WEIGHTED) ? 2 : 1;
+    constexpr int NV = (MODE == PD_MODE_WEIGHTED) ? 4 : 1;
     __shared__ int s_job;
     __shared__ double s_q[K];
+    __shared__ double s_part[PD_WARPS * NV * K];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const int n_jobs = *n_jobs_ptr;
+    double *part = s_part + warp * NV * K;
     for (;;) {
         if (threadIdx.x == 0) s_job = atomicAdd(counter, 1);
         __syncthreads();
@@ -657,27 +709,27 @@ __global__ void __launch_bounds__(PD_THREADS) pd_pairs_fp64(const PdJob *__restr
             }
         }
 
-        double *slot = rq.slots + (jb.slot + warp) * static_cast<int64_t>(K) *
-                                      (MODE == PD_MODE_WEIGHTED ? 4 : 1);
         const double wi = ivalid ? pi.w : 0.0;
 #pragma unroll
         for (int k = 0; k < K; ++k) {
             const double t0 = warp_sum(acc[0][k]);
             if (MODE == PD_MODE_CLASS) {
-                if (lane == (k & 31)) slot[k] = t0;
+                if (lane == (k & 31)) part[k] = t0;
             } else {
                 const double ti = warp_sum(wi * acc[0][k]);
                 const double tj = warp_sum(acc[NACC - 1][k]);
                 const double tij = warp_sum(wi * acc[NACC - 1][k]);
                 if (lane == (k & 31)) {
-                    slot[k] = t0;
-                    slot[K + k] = ti;
-                    slot[2 * K + k] = tj;
-                    slot[3 * K + k] = tij;
+                    part[k] = t0;
+                    part[K + k] = ti;
+                    part[2 * K + k] = tj;
+                    part[3 * K + k] = tij;
                 }
             }
         }
-        __syncthreads();  // s_q is rewritten by the next tile
+        __syncthreads();  // every warp's partial sums are complete
+        merge_tile_slots(s_part, NV * K, jb.slot, rq.slots, false, false);
+        __syncthreads();  // s_q, s_part and s_job are rewritten by the next tile
     }
 }
 

@@ -12,31 +12,6 @@
 
 namespace pd {
 
-uint64_t Plan::device_bytes() const {
-    const uint64_t atoms = static_cast<uint64_t>(n_pad) * n_frames *
-                           (precision == PD_FP64 ? sizeof(double4) : sizeof(float4));
-    const uint64_t xyz_in = static_cast<uint64_t>(n_atoms) * 3 * n_frames * sizeof(double);
-    const uint64_t tables = static_cast<uint64_t>(n_species) * nq * 2 * sizeof(double) +
-                            static_cast<uint64_t>(nq) * 2 * sizeof(double) +
-                            static_cast<uint64_t>(n_atoms) * sizeof(double);
-    const uint64_t layout = static_cast<uint64_t>(n_pad) * sizeof(int32_t) +
-                            gvalid.size() * sizeof(int32_t) +
-                            cls.size() * sizeof(PdClassDev) + pairs.size() * sizeof(PdPairDev);
-    const uint64_t jb = jobs.size() * sizeof(PdJob);
-    const uint64_t slots = static_cast<uint64_t>(slots_per_frame) * n_frames * nv * tun.K *
-                           sizeof(double);
-    const uint64_t lists = (lptr.size() + lidx.size()) * sizeof(int64_t);
-    const uint64_t sums = static_cast<uint64_t>(n_frames) * nv * n_pairs * nq * sizeof(double);
-    const uint64_t terms = static_cast<uint64_t>(n_frames + 1) * 6 * nq * sizeof(double);
-    const uint64_t misc = static_cast<uint64_t>(n_frames) * 5 * sizeof(double) + 4096;
-    const uint64_t latt = lat.empty() ? 0
-                                      : lat.size() * sizeof(PdLatDev) +
-                                            lat_tiles.size() * sizeof(PdLatTile) +
-                                            static_cast<uint64_t>(n_pad) * 16 +
-                                            static_cast<uint64_t>(lat_bins) * 8;
-    return atoms + xyz_in + tables + layout + jb + slots + lists + sums + terms + misc + latt;
-}
-
 int validate_request(const pd_request *req, bool device_pointers, std::string &msg) {
     if (!req) {
         msg = "request is NULL";
@@ -70,8 +45,8 @@ int validate_request(const pd_request *req, bool device_pointers, std::string &m
         msg = "ff_water is required when hyd_weights is given";
         return PD_EINVAL;
     }
-    if (req->flags != 0) {
-        msg = "flags must be 0";
+    if ((req->flags & ~PD_FLAG_TEST_EXPIRED_WAIT) != 0) {
+        msg = "flags must be 0 (or PD_FLAG_TEST_EXPIRED_WAIT)";
         return PD_EINVAL;
     }
     if (req->n_lattices > PD_MAX_LATTICES || (req->n_lattices && !req->lattices)) {
@@ -233,6 +208,7 @@ int build_plan(const pd_request *req, const uint32_t *species, const double *w,
     P.precision = static_cast<int>(req->precision);
     P.has_exc = req->ff_excluded != nullptr;
     P.has_hyd = req->hyd_weights != nullptr;
+    P.test_expire = (req->flags & PD_FLAG_TEST_EXPIRED_WAIT) != 0;
     P.tun = tun;
     if (!valid_q_block(P.precision, tun.K) || tun.TJ < 32 || tun.TJ % 32 != 0 ||
         tun.NP < 1 || tun.NP > 4) {
@@ -459,19 +435,39 @@ int build_plan(const pd_request *req, const uint32_t *species, const double *w,
         }
     }
     P.jobs_per_frame = static_cast<int64_t>(tiles.size()) * P.nqb;
-    P.slots_per_frame = P.jobs_per_frame * PD_WARPS;
     if (P.jobs_per_frame * P.n_frames > (int64_t{1} << 31) - 1) {
         msg = "too many tiles for one launch; use a larger j chunk";
         return PD_EINVAL;
     }
-    // Reduction lists: (pair, q-block) -> slots in creation order.
+    // Slots: the warps of one class in an i-block share one slot (the kernel
+    // adds them in warp order at the end of the tile); a padding warp (no
+    // valid atom, all-zero sums) joins slot 0. Reduction lists: (pair,
+    // q-block) -> slots in creation order.
     std::vector<std::vector<int64_t>> lists(static_cast<size_t>(P.n_pairs) * P.nqb);
     std::vector<PdJob> frame_jobs;
     frame_jobs.reserve(P.jobs_per_frame);
     uint64_t covered = 0;
-    int64_t jl = 0;
+    int64_t next_slot = 0;
     for (const Tile &t : tiles) {
-        for (int qb = 0; qb < P.nqb; ++qb, ++jl) {
+        int rel[PD_WARPS];
+        int cls_of_slot[PD_WARPS];
+        int nslot = 0;
+        int64_t map = 0;
+        for (int wv = 0; wv < PD_WARPS; ++wv) {
+            const int g = t.i0 / PD_GRANULE + wv;
+            const int a = P.gvalid[g] > 0 ? P.gclass[g] : -1;
+            int s = -1;
+            for (int u = 0; u < nslot && s < 0; ++u)
+                if (cls_of_slot[u] == a) s = u;
+            if (s < 0 && a < 0 && nslot > 0) s = 0;  // padding joins slot 0
+            if (s < 0) {
+                s = nslot;
+                cls_of_slot[nslot++] = a;
+            }
+            rel[wv] = s;
+            map |= static_cast<int64_t>(s) << (PD_SLOT_MAP_SHIFT + 2 * wv);
+        }
+        for (int qb = 0; qb < P.nqb; ++qb) {
             PdJob jb{};
             jb.req = 0;
             jb.frame = 0;
@@ -479,8 +475,9 @@ int build_plan(const pd_request *req, const uint32_t *species, const double *w,
             jb.j0 = t.j0;
             jb.j1 = t.j1;
             jb.qb = qb;
-            jb.slot = jl * PD_WARPS;
+            jb.slot = next_slot | map;
             frame_jobs.push_back(jb);
+            bool listed[PD_WARPS] = {false, false, false, false};
             for (int wv = 0; wv < PD_WARPS; ++wv) {
                 const int g = t.i0 / PD_GRANULE + wv;
                 const int a = P.gclass[g];
@@ -489,8 +486,11 @@ int build_plan(const pd_request *req, const uint32_t *species, const double *w,
                 const int64_t ilo = static_cast<int64_t>(g) * PD_GRANULE;
                 const int64_t ihi = ilo + P.gvalid[g];  // exclusive
                 if (t.j1 - 1 <= ilo) continue;          // every j <= every i
-                lists[static_cast<size_t>(pair_index[a * c + t.cls]) * P.nqb + qb].push_back(
-                    jl * PD_WARPS + wv);
+                if (!listed[rel[wv]]) {
+                    lists[static_cast<size_t>(pair_index[a * c + t.cls]) * P.nqb + qb].push_back(
+                        next_slot + rel[wv]);
+                    listed[rel[wv]] = true;
+                }
                 if (qb == 0 && count_pairs) {
                     for (int64_t i = ilo; i < ihi; ++i) {
                         const int64_t lo = std::max<int64_t>(t.j0, i + 1);
@@ -498,7 +498,13 @@ int build_plan(const pd_request *req, const uint32_t *species, const double *w,
                     }
                 }
             }
+            next_slot += nslot;
         }
+    }
+    P.slots_per_frame = next_slot;
+    if (P.slots_per_frame * P.n_frames >= (int64_t{1} << (PD_SLOT_MAP_SHIFT - 1))) {
+        msg = "too many tile slots for one request";
+        return PD_EINVAL;
     }
     for (const PdLatDev &d : P.lat)
         covered += static_cast<uint64_t>(d.n) * static_cast<uint64_t>(d.n - 1) / 2;

@@ -37,6 +37,7 @@ struct Plan {
     bool has_exc = false, has_hyd = false;
     int mode = PD_MODE_CLASS;
     int nv = 1;  // values per slot entry: 1 (class) or 4 (weighted)
+    bool test_expire = false;  // PD_FLAG_TEST_EXPIRED_WAIT
     Tuning tun;
     double qmin = 0, qmax = 0, dq = 0;
     std::vector<double> qv;
@@ -65,9 +66,6 @@ struct Plan {
     std::vector<PdLatDev> lat;
     std::vector<PdLatTile> lat_tiles;
     int64_t lat_bins = 0;
-
-    // device memory the plan needs, in bytes
-    uint64_t device_bytes() const;
 };
 
 // Validate a request; fills msg and returns a PD_E* code on failure.

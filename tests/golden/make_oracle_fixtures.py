@@ -86,6 +86,9 @@ def main(argv=None):
     ap.add_argument("--threads", type=int, default=0, help="oracle threads (0: all cores)")
     ap.add_argument("--q-index", default=None,
                     help="comma-separated grid indices (ellipsoid100k only)")
+    ap.add_argument("--append", action="store_true",
+                    help="ellipsoid100k: add the points to an existing fixture of the same "
+                         "inputs (the subset can be computed in several runs)")
     args = ap.parse_args(argv)
     if args.which == "sphere10k":
         w = workloads.sphere_solvent_10k("fp64")
@@ -93,7 +96,24 @@ def main(argv=None):
     else:
         qi = DEFAULT_100K if args.q_index is None else [int(s) for s in args.q_index.split(",")]
         w = workloads.ellipsoid_solvent_100k("fp64")
-        p = write("oracle_ellipsoid_solvent_100k.json", w, np.array(qi), args.threads)
+        name = "oracle_ellipsoid_solvent_100k.json"
+        old = None
+        if args.append and (HERE / name).exists():
+            old = json.loads((HERE / name).read_text())
+            if old["input_sha256"] != request_digest(w.request):
+                sys.exit("the existing fixture was made from other inputs")
+            qi = [i for i in qi if i not in old["q_index"]]
+        p = write(name, w, np.array(qi), args.threads)
+        if old is not None:
+            new = json.loads(p.read_text())
+            idx = old["q_index"] + new["q_index"]
+            cols = [list(r_old) + list(r_new)
+                    for r_old, r_new in zip(old["oracle_terms"], new["oracle_terms"])]
+            order = np.argsort(idx, kind="stable")
+            new["q_index"] = [idx[k] for k in order]
+            new["oracle_terms"] = [[row[k] for k in order] for row in cols]
+            new["oracle_seconds"] = round(old["oracle_seconds"] + new["oracle_seconds"], 1)
+            p.write_text(json.dumps(new, indent=None) + "\n")
     print(p)
 
 

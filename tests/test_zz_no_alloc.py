@@ -110,7 +110,7 @@ def test_noalloc_trajectory_mean_matches_pd_solve(default_ctx):
 def test_noalloc_refuses_requests_beyond_the_scratch():
     """Host-side check, before any device work: no GPU needed."""
     rng = np.random.default_rng(3)
-    n, nq = 100000, 1000
+    n, nq = 200000, 1000
     req = DebyeRequest(rng.uniform(-60, 60, (n, 3)), rng.integers(0, 4, n).astype(np.uint32),
                        rng.uniform(1, 8, (4, nq)), rng.uniform(0.5, 2, (4, nq)),
                        np.where(rng.random(n) < 0.3, 1.2, 0.0), rng.uniform(5, 10, nq),
@@ -123,9 +123,9 @@ def test_noalloc_refuses_requests_beyond_the_scratch():
 
 
 def test_noalloc_size_guide_holds():
-    """Host-only: the header's guide — an FP32 solve of 40,000 atoms with
-    solvent at nq = 500 fits the fixed scratch, 100,000 atoms at nq = 1,000
-    does not — checked on the layout the entry point computes."""
+    """Host-only: the header's guide — an FP32 solve of 100,000 atoms with
+    solvent at nq = 1,000 fits the fixed scratch, 200,000 atoms at nq = 1,000
+    do not — checked on the layout the entry point computes."""
     def need(n, nq):
         rng = np.random.default_rng(n)
         req = DebyeRequest(rng.uniform(-50, 50, (n, 3)), rng.integers(0, 4, n).astype(np.uint32),
@@ -137,8 +137,8 @@ def test_noalloc_size_guide_holds():
         _lib.check(_lib.lib().pd_request_device_bytes(None, C.byref(r), 0, C.byref(out)), None,
                    "pd_request_device_bytes")
         return out.value
-    assert need(40_000, 500) <= _lib.PD_NOALLOC_SCRATCH_BYTES
-    assert need(100_000, 1000) > _lib.PD_NOALLOC_SCRATCH_BYTES
+    assert need(100_000, 1000) <= _lib.PD_NOALLOC_SCRATCH_BYTES
+    assert need(200_000, 1000) > _lib.PD_NOALLOC_SCRATCH_BYTES
 
 
 def test_noalloc_rejects_missing_buffers():
