@@ -15,7 +15,7 @@ produce them.
 import numpy as np
 import pytest
 
-from conftest import load_golden, request_digest, term_errors
+from conftest import GOLDEN, load_golden, request_digest, term_errors
 from pripps_b200 import workloads
 from pripps_b200.debye import solve
 
@@ -29,6 +29,8 @@ FIXTURES = {
 
 def _fixture(name):
     fname, make = FIXTURES[name]
+    if not (GOLDEN / fname).exists():
+        pytest.skip(f"{fname} not generated (tests/golden/make_oracle_fixtures.py)")
     return load_golden(fname), make
 
 
