@@ -314,17 +314,46 @@ int pd_combine(const double *terms, uint64_t nq, double volume_scale,
  * thread ("" if none); NULL ctx gives the last context-free failure. */
 const char *pd_last_error(pd_ctx *ctx);
 
-/* Kernel-shape choice for the (n_atoms, nq, precision) bucket (powers of two
- * of n_atoms and nq): the q-block length K of the recurrence (FP32: 32, 64,
- * 96, 128; FP64: 16, 32), the atom-chunk length of a tile (multiple of 32)
- * and the pairs each thread advances together (FP32: 2 or 4). pd_autotune
- * times the candidates on a synthetic globule of the bucket and stores the
- * fastest; pd_get_tuning is host-only. */
+/* Kernel shapes. Every solve, plan, stream and request of the loop picks
+ * its shape — the q-block length K of the recurrence (FP32: 32, 64, 96, 128,
+ * 160, 192; FP64: 16, 32), the atom-chunk length of a tile (multiple of 32)
+ * and the pairs each thread advances together (FP32: 1, 2 or 4) — from the
+ * context's tuning table by the request's bucket: (precision, accumulation
+ * mode (class or weighted), one frame or several, floor(log2 n_atoms),
+ * floor(log2 nq)); a bucket without an entry takes a default shape. No
+ * reference counterpart (the reference has one CPU loop shape).
+ *
+ * pd_ctx_create loads the table from the file named by the environment
+ * variable PRIPPS_DEBYE_TUNING (where the autotuner then also saves its
+ * results), else from data/tuning_b200.txt beside the library when present.
+ * The file is text, one bucket per line:
+ *   <fp32|fp64> <class|weighted> <single|frames> <log2 atoms> <log2 nq>
+ *   <q_block> <j_chunk> <pairs_per_thread> <ms>
+ *
+ * pd_autotune_request times every candidate shape on the caller's own
+ * request (its structure, solvent model and grid; no lattice sets), each
+ * timed execution after an L2 flush, stores the fastest for the request's
+ * bucket and returns it with its time; pd_autotune does the same on a
+ * synthetic solvent globule of n_atoms atoms (class mode, one frame). Both
+ * run on the context's stream: do not overlap them with other work on the
+ * context. pd_get_tuning / pd_set_tuning read and write the class-mode,
+ * one-frame bucket of (n_atoms, nq, precision); pd_tuning_lookup reports the
+ * shape a request would get and whether it came from the table (host-only;
+ * ctx may be NULL: defaults). pd_tuning_load adds a file's entries to the
+ * context's table, pd_tuning_save writes the table; pd_tuning_check parses a
+ * tuning file without a context (host-only) and counts its entries. */
 int pd_get_tuning(pd_ctx *ctx, uint64_t n_atoms, uint64_t nq, uint32_t precision,
                   uint32_t *q_block, uint32_t *j_chunk, uint32_t *pairs_per_thread);
 int pd_set_tuning(pd_ctx *ctx, uint64_t n_atoms, uint64_t nq, uint32_t precision,
                   uint32_t q_block, uint32_t j_chunk, uint32_t pairs_per_thread);
 int pd_autotune(pd_ctx *ctx, uint64_t n_atoms, uint64_t nq, uint32_t precision);
+int pd_autotune_request(pd_ctx *ctx, const pd_request *req, uint32_t *q_block,
+                        uint32_t *j_chunk, uint32_t *pairs_per_thread, double *ms);
+int pd_tuning_lookup(pd_ctx *ctx, const pd_request *req, uint32_t *q_block, uint32_t *j_chunk,
+                     uint32_t *pairs_per_thread, int *from_table);
+int pd_tuning_load(pd_ctx *ctx, const char *path);
+int pd_tuning_save(pd_ctx *ctx, const char *path);
+int pd_tuning_check(const char *path, uint64_t *n_entries);
 
 /* Host-only planning report for a request (no device work): number of atom
  * classes (species × hydration weight), padded atom count, tiles launched and

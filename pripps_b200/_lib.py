@@ -123,6 +123,12 @@ SIGNATURES = {
     "pd_set_tuning": (C.c_int, [_P, C.c_uint64, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32,
                                 C.c_uint32]),
     "pd_autotune": (C.c_int, [_P, C.c_uint64, C.c_uint64, C.c_uint32]),
+    "pd_autotune_request": (C.c_int, [_P, C.POINTER(PdRequest), _U32P, _U32P, _U32P, _D]),
+    "pd_tuning_lookup": (C.c_int, [_P, C.POINTER(PdRequest), _U32P, _U32P, _U32P,
+                                   C.POINTER(C.c_int)]),
+    "pd_tuning_load": (C.c_int, [_P, C.c_char_p]),
+    "pd_tuning_save": (C.c_int, [_P, C.c_char_p]),
+    "pd_tuning_check": (C.c_int, [C.c_char_p, _U64P]),
     "pd_plan_inspect": (C.c_int, [_P, C.POINTER(PdRequest), _U64P, _U64P, _U64P, _U64P]),
     "pd_request_device_bytes": (C.c_int, [_P, C.POINTER(PdRequest), C.c_int, _U64P]),
     "pd_measure_fp32_peak": (C.c_int, [_P, _D, _D]),

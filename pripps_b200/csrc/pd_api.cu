@@ -26,7 +26,10 @@
 #include "pd_common.h"
 #include "pd_kernels.h"
 #include "pd_plan.h"
+#include "pd_tuning.h"
 #include "pripps_debye.h"
+
+#include <dlfcn.h>
 
 using pd::Plan;
 using pd::Tuning;
@@ -173,7 +176,8 @@ struct pd_ctx {
     PinnedPool pinned;              // staging images of planned requests
 
     std::mutex mu;  // tuning table, per-thread errors
-    std::map<std::tuple<int, int, int>, Tuning> tuning;
+    pd::TuneTable tuning;     // kernel shape per request bucket
+    std::string tuning_path;  // file the autotuner's results are saved to ("" = none)
     std::unordered_map<std::thread::id, std::string> errors;
     std::mutex solve_mu;  // serialises blocking solves on `stream`
 
@@ -236,19 +240,29 @@ struct DevPlan {
     }
 };
 
-Tuning tuning_for(pd_ctx *ctx, int64_t n, int64_t nq, int precision, int64_t n_frames = 1) {
-    const int nb = static_cast<int>(std::floor(std::log2(static_cast<double>(std::max<int64_t>(n, 1)))));
-    const int qb = static_cast<int>(std::floor(std::log2(static_cast<double>(std::max<int64_t>(nq, 1)))));
+// Kernel shape for a request bucket: the context's tuning table entry (the
+// autotuner's measurement, loaded from a tuning file or set by hand), else
+// the default shape.
+Tuning tuning_for(pd_ctx *ctx, int64_t n, int64_t nq, int precision, int64_t n_frames, int mode,
+                  bool *from_table = nullptr) {
+    if (from_table) *from_table = false;
     if (ctx) {
         std::lock_guard<std::mutex> g(ctx->mu);
-        auto it = ctx->tuning.find(std::make_tuple(precision, nb, qb));
+        auto it = ctx->tuning.find(pd::tune_key(n, nq, precision, mode, n_frames));
         if (it != ctx->tuning.end()) {
-            Tuning t = it->second;
-            if (precision != PD_FP64 && nq <= 32) t.K = 32;
-            return t;
+            if (from_table) *from_table = true;
+            return it->second.t;
         }
     }
     return pd::default_tuning(n, nq, precision, n_frames);
+}
+
+Tuning tuning_for_request(pd_ctx *ctx, const pd_request *req, const uint32_t *species,
+                          const double *weights, bool *from_table = nullptr) {
+    return tuning_for(ctx, static_cast<int64_t>(req->n_atoms), static_cast<int64_t>(req->nq),
+                      static_cast<int>(req->precision),
+                      static_cast<int64_t>(req->n_frames ? req->n_frames : 1),
+                      pd::request_mode(req, species, weights), from_table);
 }
 
 void free_devplan(pd_ctx *ctx, DevPlan &dp, cudaStream_t st) {
@@ -346,11 +360,9 @@ constexpr int kBudgetWait = -100;  // internal: does not fit the budget right no
 
 // Host planning only: tiles, lists and the device layout.
 int plan_host(pd_ctx *ctx, const pd_request *req, const uint32_t *species, const double *weights,
-              bool host_xyz, DevPlan &dp) {
+              bool host_xyz, DevPlan &dp, const Tuning *force = nullptr) {
     std::string msg;
-    Tuning tun = tuning_for(ctx, static_cast<int64_t>(req->n_atoms),
-                            static_cast<int64_t>(req->nq), static_cast<int>(req->precision),
-                            static_cast<int64_t>(req->n_frames));
+    const Tuning tun = force ? *force : tuning_for_request(ctx, req, species, weights);
     int rc = pd::build_plan(req, species, weights, tun, dp.P, msg);
     if (rc != PD_OK) {
         ctx->set_error(msg);
@@ -405,8 +417,9 @@ int plan_device(pd_ctx *ctx, const pd_request *req, DevPlan &dp, cudaStream_t st
 }
 
 int create_devplan(pd_ctx *ctx, const pd_request *req, const uint32_t *species,
-                   const double *weights, bool host_xyz, DevPlan &dp, cudaStream_t st) {
-    int rc = plan_host(ctx, req, species, weights, host_xyz, dp);
+                   const double *weights, bool host_xyz, DevPlan &dp, cudaStream_t st,
+                   const Tuning *force = nullptr) {
+    int rc = plan_host(ctx, req, species, weights, host_xyz, dp, force);
     if (rc) return rc;
     return plan_device(ctx, req, dp, st, false);
 }
@@ -1106,6 +1119,36 @@ int pd_ctx_create(int device, uint64_t mem_budget_bytes, pd_ctx **out) {
         delete ctx;
         return PD_EDEVICE;
     }
+    // Tuning table: the file named by PRIPPS_DEBYE_TUNING (the autotuner
+    // also saves its results there), else the table shipped beside the
+    // library (data/tuning_b200.txt). A missing file leaves the defaults; a
+    // malformed one fails the context.
+    {
+        std::string path;
+        const char *env = std::getenv("PRIPPS_DEBYE_TUNING");
+        if (env && *env) {
+            path = env;
+            ctx->tuning_path = path;
+        } else {
+            Dl_info info{};
+            if (dladdr(reinterpret_cast<void *>(&pd_ctx_create), &info) && info.dli_fname) {
+                std::string so = info.dli_fname;
+                const size_t slash = so.rfind('/');
+                path = (slash == std::string::npos ? std::string(".") : so.substr(0, slash)) +
+                       "/data/tuning_b200.txt";
+            }
+        }
+        std::string msg;
+        const int trc = path.empty() ? PD_ENOTFOUND : pd::load_tuning(path, ctx->tuning, msg);
+        if (trc != PD_OK && trc != PD_ENOTFOUND) {
+            std::lock_guard<std::mutex> g(g_err_mu);
+            g_err = msg;
+            cudaStreamDestroy(ctx->stream);
+            if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
+            delete ctx;
+            return trc;
+        }
+    }
     *out = ctx;
     return PD_OK;
 }
@@ -1182,7 +1225,16 @@ int pd_solve(pd_ctx *ctx, const pd_request *req, double *out_terms) {
     return rc;
 }
 
+namespace {
+int plan_create_impl(pd_ctx *ctx, const pd_request *req, pd_plan **out, const Tuning *force);
+}
+
 int pd_plan_create(pd_ctx *ctx, const pd_request *req, pd_plan **out) {
+    return plan_create_impl(ctx, req, out, nullptr);
+}
+
+namespace {
+int plan_create_impl(pd_ctx *ctx, const pd_request *req, pd_plan **out, const Tuning *force) {
     if (!ctx || !out || !req) return PD_EINVAL;
     *out = nullptr;
     // Coordinates arrive at execute time; validate the rest on the host.
@@ -1204,7 +1256,7 @@ int pd_plan_create(pd_ctx *ctx, const pd_request *req, pd_plan **out) {
     std::lock_guard<std::mutex> g(ctx->solve_mu);
     cudaSetDevice(ctx->device);
     auto *p = new pd_plan();
-    rc = create_devplan(ctx, &r, r.species, r.hyd_weights, false, p->dp, ctx->stream);
+    rc = create_devplan(ctx, &r, r.species, r.hyd_weights, false, p->dp, ctx->stream, force);
     if (rc == PD_OK) {
         cudaError_t e = cudaStreamSynchronize(ctx->stream);
         if (e != cudaSuccess) rc = cuda_fail(ctx, e, "pd_plan_create");
@@ -1217,6 +1269,7 @@ int pd_plan_create(pd_ctx *ctx, const pd_request *req, pd_plan **out) {
     *out = p;
     return PD_OK;
 }
+}  // namespace
 
 int pd_plan_execute(pd_ctx *ctx, pd_plan *plan, const double *xyz_dev, double *out_terms_dev,
                     void *stream) {
@@ -1348,9 +1401,7 @@ int pd_plan_tiles(pd_ctx *ctx, const pd_request *req, uint32_t rank, uint32_t wo
         if (ctx) ctx->set_error(msg);
         return rc;
     }
-    Tuning tun = tuning_for(ctx, static_cast<int64_t>(req->n_atoms), static_cast<int64_t>(req->nq),
-                            static_cast<int>(req->precision),
-                            static_cast<int64_t>(req->n_frames));
+    Tuning tun = tuning_for_request(ctx, req, req->species, req->hyd_weights);
     Plan P;
     rc = pd::build_plan(req, req->species, req->hyd_weights, tun, P, msg);
     if (rc) {
@@ -1505,7 +1556,7 @@ int pd_combine(const double *terms, uint64_t nq, double vs, double c, double *to
 int pd_get_tuning(pd_ctx *ctx, uint64_t n_atoms, uint64_t nq, uint32_t precision,
                   uint32_t *q_block, uint32_t *j_chunk, uint32_t *pairs_per_thread) {
     Tuning t = tuning_for(ctx, static_cast<int64_t>(n_atoms), static_cast<int64_t>(nq),
-                          static_cast<int>(precision));
+                          static_cast<int>(precision), 1, PD_MODE_CLASS);
     if (q_block) *q_block = static_cast<uint32_t>(t.K);
     if (j_chunk) *j_chunk = static_cast<uint32_t>(t.TJ);
     if (pairs_per_thread) *pairs_per_thread = static_cast<uint32_t>(t.NP);
@@ -1515,33 +1566,177 @@ int pd_get_tuning(pd_ctx *ctx, uint64_t n_atoms, uint64_t nq, uint32_t precision
 int pd_set_tuning(pd_ctx *ctx, uint64_t n_atoms, uint64_t nq, uint32_t precision, uint32_t q_block,
                   uint32_t j_chunk, uint32_t pairs_per_thread) {
     if (!ctx) return PD_EINVAL;
-    const int np = precision == PD_FP64 ? 1 : static_cast<int>(pairs_per_thread);
-    if (!pd::valid_q_block(static_cast<int>(precision), static_cast<int>(q_block)) ||
-        j_chunk < 32 || j_chunk % 32 != 0 ||
-        (precision != PD_FP64 &&
-         !pd::valid_shape(static_cast<int>(precision), PD_MODE_CLASS, static_cast<int>(q_block), np))) {
-        ctx->set_error("invalid tuning");
-        return PD_EINVAL;
-    }
-    const int nb = static_cast<int>(std::floor(std::log2(static_cast<double>(std::max<uint64_t>(n_atoms, 1)))));
-    const int qb = static_cast<int>(std::floor(std::log2(static_cast<double>(std::max<uint64_t>(nq, 1)))));
-    std::lock_guard<std::mutex> g(ctx->mu);
     Tuning t;
     t.K = static_cast<int>(q_block);
     t.TJ = static_cast<int>(j_chunk);
-    t.NP = np;
-    ctx->tuning[std::make_tuple(static_cast<int>(precision), nb, qb)] = t;
+    t.NP = precision == PD_FP64 ? 1 : static_cast<int>(pairs_per_thread);
+    if (precision > PD_FP64 || !pd::valid_tuning(static_cast<int>(precision), PD_MODE_CLASS, t)) {
+        ctx->set_error("invalid tuning");
+        return PD_EINVAL;
+    }
+    std::lock_guard<std::mutex> g(ctx->mu);
+    ctx->tuning[pd::tune_key(static_cast<int64_t>(n_atoms), static_cast<int64_t>(nq),
+                             static_cast<int>(precision), PD_MODE_CLASS, 1)] = pd::TuneEntry{t, 0.0};
+    return PD_OK;
+}
+
+namespace {
+
+// Candidate shapes of a bucket: the instantiated (q block, pairs per thread)
+// shapes of its precision and mode, each with j chunks of about N/32 .. N/4
+// atoms (powers of two, 256 .. 16,384), and the default shape.
+std::vector<Tuning> tune_candidates(const pd_request *req, int mode) {
+    const int precision = static_cast<int>(req->precision);
+    const int64_t n = static_cast<int64_t>(req->n_atoms), nq = static_cast<int64_t>(req->nq);
+    std::vector<std::pair<int, int>> shapes;
+    if (precision == PD_FP64)
+        shapes = {{16, 1}, {32, 1}};
+    else if (mode == PD_MODE_WEIGHTED)
+        shapes = {{32, 2}, {64, 2}};
+    else if (nq <= 32)
+        shapes = {{32, 4}};
+    else
+        shapes = {{64, 2}, {64, 4}, {96, 2}, {128, 1}, {128, 2}, {128, 4}};
+    std::vector<int> tjs;
+    for (int d : {32, 16, 8, 4}) {
+        int tj = 256;
+        while (tj < n / d && tj < 16384) tj <<= 1;
+        if (std::find(tjs.begin(), tjs.end(), tj) == tjs.end()) tjs.push_back(tj);
+    }
+    std::vector<Tuning> out;
+    const Tuning def = pd::default_tuning(n, nq, precision, static_cast<int64_t>(req->n_frames));
+    out.push_back(def);
+    for (auto sh : shapes)
+        for (int tj : tjs) {
+            Tuning t;
+            t.K = sh.first;
+            t.NP = sh.second;
+            t.TJ = tj;
+            if (!pd::valid_tuning(precision, mode, t)) continue;
+            bool dup = false;
+            for (const Tuning &o : out) dup |= o.K == t.K && o.NP == t.NP && o.TJ == t.TJ;
+            if (!dup) out.push_back(t);
+        }
+    return out;
+}
+
+// Times every candidate shape on the caller's request and keeps the fastest
+// for the request's bucket. Each timed execution starts with L2 flushed (a
+// 256 MiB write), as a stream of independent requests would meet it.
+int autotune_request(pd_ctx *ctx, const pd_request *req, Tuning *best_out, double *best_ms) {
+    std::string msg;
+    int rc = pd::validate_request(req, false, msg);
+    if (rc) {
+        ctx->set_error(msg);
+        return rc;
+    }
+    if (req->n_lattices) {
+        ctx->set_error("pd_autotune_request: tune the request without its lattice sets");
+        return PD_EINVAL;
+    }
+    const int mode = pd::request_mode(req, req->species, req->hyd_weights);
+    const std::vector<Tuning> cands = tune_candidates(req, mode);
+    cudaSetDevice(ctx->device);
+    cudaStream_t st = ctx->stream;
+    const uint64_t nf = req->n_frames ? req->n_frames : 1;
+    const size_t nxyz = static_cast<size_t>(req->n_atoms) * 3 * nf;
+    const size_t flush_bytes = size_t{256} << 20;
+    double *xyz_dev = nullptr, *out_dev = nullptr;
+    char *flush = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaError_t e = cudaMallocFromPoolAsync(reinterpret_cast<void **>(&xyz_dev), nxyz * 8, ctx->pool, st);
+    if (e == cudaSuccess)
+        e = cudaMallocFromPoolAsync(reinterpret_cast<void **>(&out_dev), 6 * req->nq * 8, ctx->pool, st);
+    if (e == cudaSuccess)
+        e = cudaMallocFromPoolAsync(reinterpret_cast<void **>(&flush), flush_bytes, ctx->pool, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(xyz_dev, req->xyz, nxyz * 8, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaEventCreate(&e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&e1);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    double best = 1e300;
+    Tuning best_t = cands.front();
+    for (size_t c = 0; c < cands.size() && e == cudaSuccess; ++c) {
+        pd_plan *plan = nullptr;
+        if (plan_create_impl(ctx, req, &plan, &cands[c]) != PD_OK) continue;
+        // warm-up, then timed executions (one when a run takes over 0.25 s)
+        bool ok = pd_plan_execute(ctx, plan, xyz_dev, out_dev, st) == PD_OK;
+        double total = 0.0;
+        int reps = 0;
+        for (int rep = 0; rep < 3 && ok; ++rep) {
+            ok = cudaMemsetAsync(flush, rep + 1, flush_bytes, st) == cudaSuccess &&
+                 cudaEventRecord(e0, st) == cudaSuccess &&
+                 pd_plan_execute(ctx, plan, xyz_dev, out_dev, st) == PD_OK &&
+                 cudaEventRecord(e1, st) == cudaSuccess && cudaEventSynchronize(e1) == cudaSuccess;
+            float ms = 0.0f;
+            if (ok) ok = cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess;
+            if (!ok) break;
+            total += ms;
+            ++reps;
+            if (ms > 250.0f && reps >= 1) break;
+        }
+        pd_plan_destroy(ctx, plan);
+        if (ok && reps > 0 && total / reps < best) {
+            best = total / reps;
+            best_t = cands[c];
+        }
+    }
+    if (xyz_dev) cudaFreeAsync(xyz_dev, st);
+    if (out_dev) cudaFreeAsync(out_dev, st);
+    if (flush) cudaFreeAsync(flush, st);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    const cudaError_t e2 = cudaStreamSynchronize(st);
+    if (e == cudaSuccess) e = e2;
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "pd_autotune_request");
+    if (best >= 1e300) {
+        ctx->set_error("pd_autotune_request: no candidate shape ran");
+        return PD_EDEVICE;
+    }
+    std::string path;
+    pd::TuneTable snapshot;
+    {
+        std::lock_guard<std::mutex> g(ctx->mu);
+        ctx->tuning[pd::tune_key(static_cast<int64_t>(req->n_atoms), static_cast<int64_t>(req->nq),
+                                 static_cast<int>(req->precision), mode,
+                                 static_cast<int64_t>(nf))] = pd::TuneEntry{best_t, best};
+        path = ctx->tuning_path;
+        if (!path.empty()) snapshot = ctx->tuning;
+    }
+    if (!path.empty() && pd::save_tuning(path, snapshot, msg) != PD_OK) {
+        ctx->set_error(msg);
+        return PD_EINVAL;
+    }
+    if (best_out) *best_out = best_t;
+    if (best_ms) *best_ms = best;
+    return PD_OK;
+}
+
+}  // namespace
+
+int pd_autotune_request(pd_ctx *ctx, const pd_request *req, uint32_t *q_block, uint32_t *j_chunk,
+                        uint32_t *pairs_per_thread, double *ms) {
+    if (!ctx || !req) return PD_EINVAL;
+    Tuning t;
+    double best = 0.0;
+    const int rc = autotune_request(ctx, req, &t, &best);
+    if (rc) return rc;
+    if (q_block) *q_block = static_cast<uint32_t>(t.K);
+    if (j_chunk) *j_chunk = static_cast<uint32_t>(t.TJ);
+    if (pairs_per_thread) *pairs_per_thread = static_cast<uint32_t>(t.NP);
+    if (ms) *ms = best;
     return PD_OK;
 }
 
 int pd_autotune(pd_ctx *ctx, uint64_t n_atoms, uint64_t nq, uint32_t precision) {
-    if (!ctx || n_atoms < 2 || nq < 1) return PD_EINVAL;
-    // Synthetic globule of the bucket's size: uniform in a sphere at the
-    // density of a protein (≈ 12 Å³ per atom), four species.
+    if (!ctx || n_atoms < 2 || nq < 1 || precision > PD_FP64) return PD_EINVAL;
+    // Synthetic solvent globule of the bucket's size: uniform in a sphere at
+    // the density of a protein (about 12 Å³ per atom), four species, the
+    // outer shell hydrated with one weight per species (class mode, as the
+    // FoXS-style surface hydration of real requests runs).
     std::mt19937_64 rng(12345);
     std::uniform_real_distribution<double> U(-1.0, 1.0);
     const double R = std::cbrt(12.0 * static_cast<double>(n_atoms) * 3.0 / (4.0 * M_PI));
-    std::vector<double> xyz(n_atoms * 3);
+    std::vector<double> xyz(n_atoms * 3), hw(n_atoms);
     std::vector<uint32_t> sp(n_atoms);
     for (uint64_t i = 0; i < n_atoms; ++i) {
         double x, y, z;
@@ -1554,72 +1749,91 @@ int pd_autotune(pd_ctx *ctx, uint64_t n_atoms, uint64_t nq, uint32_t precision) 
         xyz[3 * i + 1] = R * y;
         xyz[3 * i + 2] = R * z;
         sp[i] = static_cast<uint32_t>(i % 4);
+        const double rr = R * std::sqrt(x * x + y * y + z * z);
+        hw[i] = (rr > R - 3.0 && U(rng) < -0.3) ? 1.5 + 0.25 * sp[i] : 0.0;
     }
-    std::vector<double> ff(4 * nq, 1.0);
+    std::vector<double> ffA(4 * nq), ffC(4 * nq), ffW(nq);
+    for (uint64_t k = 0; k < nq; ++k) {
+        const double q = 0.5 * static_cast<double>(k) / static_cast<double>(nq > 1 ? nq - 1 : 1);
+        for (int s = 0; s < 4; ++s) {
+            ffA[s * nq + k] = (6.0 + s) * std::exp(-0.1 * q * q);
+            ffC[s * nq + k] = (2.0 + 0.5 * s) * std::exp(-0.4 * q * q);
+        }
+        ffW[k] = 10.0 * std::exp(-0.2 * q * q);
+    }
     pd_request rq{};
     rq.n_atoms = n_atoms;
     rq.xyz = xyz.data();
     rq.species = sp.data();
     rq.n_species = 4;
     rq.precision = precision;
-    rq.ff_atoms = ff.data();
+    rq.ff_atoms = ffA.data();
+    rq.ff_excluded = ffC.data();
+    rq.hyd_weights = hw.data();
+    rq.ff_water = ffW.data();
     rq.qmin = 0.0;
     rq.qmax = 0.5;
     rq.nq = nq;
-    std::vector<std::pair<int, int>> shapes =
-        precision == PD_FP64
-            ? std::vector<std::pair<int, int>>{{16, 1}, {32, 1}}
-            : std::vector<std::pair<int, int>>{{32, 4}, {64, 2}, {64, 4}, {96, 2}, {128, 2}, {128, 4}};
-    std::vector<int> TJs = {512, 1024, 2048, 4096, 8192};
-    double best = 1e300;
-    Tuning best_t = pd::default_tuning(static_cast<int64_t>(n_atoms), static_cast<int64_t>(nq),
-                                       static_cast<int>(precision));
-    cudaSetDevice(ctx->device);
-    cudaEvent_t e0, e1;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e1);
-    double *xyz_dev = nullptr, *out_dev = nullptr;
-    cudaError_t ae = cudaMalloc(reinterpret_cast<void **>(&xyz_dev), xyz.size() * 8);
-    if (ae == cudaSuccess) ae = cudaMalloc(reinterpret_cast<void **>(&out_dev), 6 * nq * 8);
-    if (ae == cudaSuccess)
-        ae = cudaMemcpy(xyz_dev, xyz.data(), xyz.size() * 8, cudaMemcpyHostToDevice);
-    if (ae != cudaSuccess) {
-        cudaFree(xyz_dev);
-        cudaFree(out_dev);
-        cudaEventDestroy(e0);
-        cudaEventDestroy(e1);
-        return cuda_fail(ctx, ae, "pd_autotune");
+    return autotune_request(ctx, &rq, nullptr, nullptr);
+}
+
+int pd_tuning_load(pd_ctx *ctx, const char *path) {
+    if (!ctx || !path) return PD_EINVAL;
+    pd::TuneTable tab;
+    std::string msg;
+    const int rc = pd::load_tuning(path, tab, msg);
+    if (rc) {
+        ctx->set_error(msg);
+        return rc;
     }
-    for (auto shape : shapes) {
-        const int K = shape.first, NP = shape.second;
-        if (precision != PD_FP64 && nq <= 32 && K != 32) continue;
-        for (int TJ : TJs) {
-            if (TJ > static_cast<int>(2 * n_atoms) && TJ != TJs.front()) continue;
-            pd_set_tuning(ctx, n_atoms, nq, precision, K, TJ, NP);
-            pd_plan *plan = nullptr;
-            if (pd_plan_create(ctx, &rq, &plan) != PD_OK) continue;
-            float ms = 0;
-            bool ok = pd_plan_execute(ctx, plan, xyz_dev, out_dev, ctx->stream) == PD_OK;
-            cudaEventRecord(e0, ctx->stream);
-            for (int rep = 0; rep < 2 && ok; ++rep)
-                ok = pd_plan_execute(ctx, plan, xyz_dev, out_dev, ctx->stream) == PD_OK;
-            cudaEventRecord(e1, ctx->stream);
-            if (cudaEventSynchronize(e1) != cudaSuccess) ok = false;
-            cudaEventElapsedTime(&ms, e0, e1);
-            pd_plan_destroy(ctx, plan);
-            if (ok && ms < best) {
-                best = ms;
-                best_t.K = K;
-                best_t.TJ = TJ;
-                best_t.NP = NP;
-            }
-        }
+    std::lock_guard<std::mutex> g(ctx->mu);
+    for (auto &kv : tab) ctx->tuning[kv.first] = kv.second;
+    return PD_OK;
+}
+
+int pd_tuning_save(pd_ctx *ctx, const char *path) {
+    if (!ctx || !path) return PD_EINVAL;
+    pd::TuneTable snapshot;
+    {
+        std::lock_guard<std::mutex> g(ctx->mu);
+        snapshot = ctx->tuning;
     }
-    cudaFree(xyz_dev);
-    cudaFree(out_dev);
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    return pd_set_tuning(ctx, n_atoms, nq, precision, best_t.K, best_t.TJ, best_t.NP);
+    std::string msg;
+    const int rc = pd::save_tuning(path, snapshot, msg);
+    if (rc) ctx->set_error(msg);
+    return rc;
+}
+
+int pd_tuning_lookup(pd_ctx *ctx, const pd_request *req, uint32_t *q_block, uint32_t *j_chunk,
+                     uint32_t *pairs_per_thread, int *from_table) {
+    if (!req) return PD_EINVAL;
+    std::string msg;
+    const int rc = pd::validate_request(req, false, msg);
+    if (rc) {
+        if (ctx) ctx->set_error(msg);
+        return rc;
+    }
+    bool tab = false;
+    const Tuning t = tuning_for_request(ctx, req, req->species, req->hyd_weights, &tab);
+    if (q_block) *q_block = static_cast<uint32_t>(t.K);
+    if (j_chunk) *j_chunk = static_cast<uint32_t>(t.TJ);
+    if (pairs_per_thread) *pairs_per_thread = static_cast<uint32_t>(t.NP);
+    if (from_table) *from_table = tab ? 1 : 0;
+    return PD_OK;
+}
+
+int pd_tuning_check(const char *path, uint64_t *n_entries) {
+    if (!path) return PD_EINVAL;
+    pd::TuneTable tab;
+    std::string msg;
+    const int rc = pd::load_tuning(path, tab, msg);
+    if (rc) {
+        std::lock_guard<std::mutex> g(g_err_mu);
+        g_err = msg;
+        return rc;
+    }
+    if (n_entries) *n_entries = tab.size();
+    return PD_OK;
 }
 
 int pd_plan_inspect(pd_ctx *ctx, const pd_request *req, uint64_t *n_classes, uint64_t *n_padded,
@@ -1630,9 +1844,7 @@ int pd_plan_inspect(pd_ctx *ctx, const pd_request *req, uint64_t *n_classes, uin
         if (ctx) ctx->set_error(msg);
         return rc;
     }
-    Tuning tun = tuning_for(ctx, static_cast<int64_t>(req->n_atoms), static_cast<int64_t>(req->nq),
-                            static_cast<int>(req->precision),
-                            static_cast<int64_t>(req->n_frames));
+    Tuning tun = tuning_for_request(ctx, req, req->species, req->hyd_weights);
     Plan P;
     rc = pd::build_plan(req, req->species, req->hyd_weights, tun, P, msg, /*count_pairs=*/true);
     if (rc) {
@@ -1655,9 +1867,7 @@ int pd_request_device_bytes(pd_ctx *ctx, const pd_request *req, int host_coordin
         if (ctx) ctx->set_error(msg);
         return rc;
     }
-    Tuning tun = tuning_for(ctx, static_cast<int64_t>(req->n_atoms), static_cast<int64_t>(req->nq),
-                            static_cast<int>(req->precision),
-                            static_cast<int64_t>(req->n_frames));
+    Tuning tun = tuning_for_request(ctx, req, req->species, req->hyd_weights);
     Plan P;
     rc = pd::build_plan(req, req->species, req->hyd_weights, tun, P, msg);
     if (rc) {
@@ -2304,9 +2514,7 @@ extern "C" int pd_solve_noalloc(const pd_request *req, const double *xyz_dev,
     int rc = noalloc_validate(&r, msg);
     if (rc) return noalloc_fail(rc, "pd_solve_noalloc: " + msg);
     DevPlan dp;
-    Tuning tun = tuning_for(nullptr, static_cast<int64_t>(r.n_atoms), static_cast<int64_t>(r.nq),
-                            static_cast<int>(r.precision),
-                            static_cast<int64_t>(r.n_frames));
+    Tuning tun = tuning_for_request(nullptr, &r, r.species, r.hyd_weights);
     rc = pd::build_plan(&r, r.species, r.hyd_weights, tun, dp.P, msg);
     if (rc) return noalloc_fail(rc, "pd_solve_noalloc: " + msg);
     dp.L = make_layout(dp.P, false);
