@@ -338,8 +338,10 @@ const char *pd_last_error(pd_ctx *ctx);
  * run on the context's stream: do not overlap them with other work on the
  * context. pd_get_tuning / pd_set_tuning read and write the class-mode,
  * one-frame bucket of (n_atoms, nq, precision); pd_tuning_lookup reports the
- * shape a request would get and whether it came from the table (host-only;
- * ctx may be NULL: defaults). pd_tuning_load adds a file's entries to the
+ * shape a request would get and whether it came from the table (host-only).
+ * Calls without a context (pd_solve_noalloc, and the host-only queries with
+ * ctx = NULL) use the table a new context would load, read once per
+ * process. pd_tuning_load adds a file's entries to the
  * context's table, pd_tuning_save writes the table; pd_tuning_check parses a
  * tuning file without a context (host-only) and counts its entries. */
 int pd_get_tuning(pd_ctx *ctx, uint64_t n_atoms, uint64_t nq, uint32_t precision,

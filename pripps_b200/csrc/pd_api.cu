@@ -240,16 +240,59 @@ struct DevPlan {
     }
 };
 
-// Kernel shape for a request bucket: the context's tuning table entry (the
-// autotuner's measurement, loaded from a tuning file or set by hand), else
-// the default shape.
+// The tuning table a context starts from: the file named by
+// PRIPPS_DEBYE_TUNING, else data/tuning_b200.txt beside this library.
+int load_default_tuning(pd::TuneTable &tab, bool *from_env, std::string &msg) {
+    std::string path;
+    const char *env = std::getenv("PRIPPS_DEBYE_TUNING");
+    *from_env = env && *env;
+    if (*from_env) {
+        path = env;
+    } else {
+        Dl_info info{};
+        if (dladdr(reinterpret_cast<void *>(&load_default_tuning), &info) && info.dli_fname) {
+            const std::string so = info.dli_fname;
+            const size_t slash = so.rfind('/');
+            path = (slash == std::string::npos ? std::string(".") : so.substr(0, slash)) +
+                   "/data/tuning_b200.txt";
+        }
+    }
+    if (path.empty()) return PD_ENOTFOUND;
+    return pd::load_tuning(path, tab, msg);
+}
+
+// Calls without a context (pd_solve_noalloc, host-only queries with NULL)
+// use the table a new context would load, read once per process.
+const pd::TuneTable &process_tuning() {
+    static pd::TuneTable tab;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        std::string msg;
+        bool from_env = false;
+        pd::TuneTable t;
+        if (load_default_tuning(t, &from_env, msg) == PD_OK) tab = std::move(t);
+    });
+    return tab;
+}
+
+// Kernel shape for a request bucket: the tuning table entry (the
+// autotuner's measurement, loaded from a tuning file or set by hand) of the
+// context, or of the process without one; else the default shape.
 Tuning tuning_for(pd_ctx *ctx, int64_t n, int64_t nq, int precision, int64_t n_frames, int mode,
                   bool *from_table = nullptr) {
     if (from_table) *from_table = false;
+    const pd::TuneKey key = pd::tune_key(n, nq, precision, mode, n_frames);
     if (ctx) {
         std::lock_guard<std::mutex> g(ctx->mu);
-        auto it = ctx->tuning.find(pd::tune_key(n, nq, precision, mode, n_frames));
+        auto it = ctx->tuning.find(key);
         if (it != ctx->tuning.end()) {
+            if (from_table) *from_table = true;
+            return it->second.t;
+        }
+    } else {
+        const pd::TuneTable &tab = process_tuning();
+        auto it = tab.find(key);
+        if (it != tab.end()) {
             if (from_table) *from_table = true;
             return it->second.t;
         }
@@ -1121,25 +1164,13 @@ int pd_ctx_create(int device, uint64_t mem_budget_bytes, pd_ctx **out) {
     }
     // Tuning table: the file named by PRIPPS_DEBYE_TUNING (the autotuner
     // also saves its results there), else the table shipped beside the
-    // library (data/tuning_b200.txt). A missing file leaves the defaults; a
-    // malformed one fails the context.
+    // library. A missing file leaves the defaults; a malformed one fails the
+    // context.
     {
-        std::string path;
-        const char *env = std::getenv("PRIPPS_DEBYE_TUNING");
-        if (env && *env) {
-            path = env;
-            ctx->tuning_path = path;
-        } else {
-            Dl_info info{};
-            if (dladdr(reinterpret_cast<void *>(&pd_ctx_create), &info) && info.dli_fname) {
-                std::string so = info.dli_fname;
-                const size_t slash = so.rfind('/');
-                path = (slash == std::string::npos ? std::string(".") : so.substr(0, slash)) +
-                       "/data/tuning_b200.txt";
-            }
-        }
         std::string msg;
-        const int trc = path.empty() ? PD_ENOTFOUND : pd::load_tuning(path, ctx->tuning, msg);
+        bool from_env = false;
+        const int trc = load_default_tuning(ctx->tuning, &from_env, msg);
+        if (from_env) ctx->tuning_path = std::getenv("PRIPPS_DEBYE_TUNING");
         if (trc != PD_OK && trc != PD_ENOTFOUND) {
             std::lock_guard<std::mutex> g(g_err_mu);
             g_err = msg;

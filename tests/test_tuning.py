@@ -69,6 +69,8 @@ def lookup(req, ctx=None):
 
 
 def test_lookup_without_context_is_the_default_shape():
+    if SHIPPED.exists() or os.environ.get("PRIPPS_DEBYE_TUNING"):
+        pytest.skip("a tuning table is installed")
     shape, from_table = lookup(workloads.small_globule(5000, 1, nq=300).request)
     # q block 128 with two pairs per thread from 4,000 atoms up; the j chunk
     # is halved until a solve has about six tiles per resident CTA
