@@ -251,6 +251,8 @@ def run_ours(args, ws, rank, local):
                                           C.c_uint64(), C.c_uint64())
     lib.pd_plan_info(plan, C.byref(kb), C.byref(tj), C.byref(npt), C.byref(ntile), C.byref(dbytes),
                      C.byref(ubytes))
+    from_table = C.c_int(0)
+    lib.pd_tuning_lookup(ctx.handle, C.byref(r), None, None, None, C.byref(from_table))
     xyz = torch.from_numpy(req.xyz).to(f"cuda:{local}")
     out = torch.empty((6, req.nq), dtype=torch.float64, device=f"cuda:{local}")
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
@@ -356,7 +358,10 @@ def run_ours(args, ws, rank, local):
         fp64 = {"value": pq64 / (ms64 * 1e-3), "unit": UNIT, "nq": r64.nq, "ms": ms64,
                 "fp32_over_fp64": (w.pair_q / (ms_per_step * 1e-3)) / (pq64 / (ms64 * 1e-3))}
 
-    # ---- end to end through the C ABI with host buffers
+    # ---- end to end through the C ABI with host buffers: every step plans
+    # the request on the host, uploads it and downloads the result (N = 1:
+    # the blocking pd_solve; N > 1: a plan of this rank's tiles, the
+    # coordinates from pinned memory, the all-reduce and the download)
     e2e_times = []
     res_host = None
     xyz_pinned = torch.from_numpy(req.xyz).pin_memory() if ws > 1 else None
@@ -367,9 +372,15 @@ def run_ours(args, ws, rank, local):
         if ws == 1:
             res_host = solve(req, ctx)  # pd_solve: plan, upload, kernels, download
         else:
+            pe = C.c_void_p()
+            _lib.check(lib.pd_plan_create(ctx.handle, C.byref(r), C.byref(pe)), ctx.handle)
+            _lib.check(lib.pd_plan_set_shard(ctx.handle, pe, rank, ws), ctx.handle)
             xyz.copy_(xyz_pinned, non_blocking=True)
-            execute()
+            _lib.check(lib.pd_plan_execute(ctx.handle, pe, xyz.data_ptr(), out.data_ptr(), sp),
+                       ctx.handle)
+            torch.distributed.all_reduce(out, op=torch.distributed.ReduceOp.SUM)
             res_host = out.cpu().numpy()
+            lib.pd_plan_destroy(ctx.handle, pe)
         dt = time.perf_counter() - t0
         if i > 0:
             e2e_times.append(dt)
@@ -380,6 +391,9 @@ def run_ours(args, ws, rank, local):
         e2e_ms = float(t.item())
     same = bool(np.array_equal(res_host, result_dev)) if res_host is not None else None
     lib.pd_plan_destroy(ctx.handle, plan)
+    secondary = None
+    if rank == 0 and ws == 1 and not args.no_secondary:
+        secondary = run_secondary(ctx, args, local)
 
     if rank == 0:
         mode = "class"
@@ -446,13 +460,106 @@ def run_ours(args, ws, rank, local):
             "parallelism": f"tile-sharded solve over {ws} GPUs + NCCL all-reduce" if ws > 1
                            else "1 GPU",
             "tiles": {"q_block": kb.value, "j_chunk": tj.value, "pairs_per_thread": npt.value,
-                      "tiles_per_solve": ntile.value, "device_bytes": dbytes.value},
+                      "tiles_per_solve": ntile.value, "device_bytes": dbytes.value,
+                      "shape_source": "autotuned table entry for the request's bucket"
+                                      if from_table.value else "default shape (no table entry)"},
         }
+        if secondary:
+            line["secondary"] = secondary
         print(json.dumps(line), flush=True)
     ctx.close()
     if ws > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
+
+
+def timed_workload(ctx, w, local, min_seconds=2.0):
+    """Device-resident executions of one workload, repeated until the timed
+    region lasts at least `min_seconds` (so the clock sampler sees it), L2
+    flushed before each; returns pair·q/s, ms per solve, repeats, clocks."""
+    import torch
+
+    from pripps_b200 import _lib
+    lib = _lib.lib()
+    req = w.request
+    r = req.c_struct()
+    plan = C.c_void_p()
+    _lib.check(lib.pd_plan_create(ctx.handle, C.byref(r), C.byref(plan)), ctx.handle)
+    xyz = torch.from_numpy(req.xyz).to(f"cuda:{local}")
+    out = torch.empty((6, req.nq), dtype=torch.float64, device=f"cuda:{local}")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+    stream = torch.cuda.current_stream()
+    sp = stream.cuda_stream
+
+    def execute():
+        _lib.check(lib.pd_plan_execute(ctx.handle, plan, xyz.data_ptr(), out.data_ptr(), sp),
+                   ctx.handle)
+
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for _ in range(3):
+        execute()
+        flush.zero_()
+    e0.record(stream)
+    execute()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    reps = max(3, int(np.ceil(min_seconds / max(e0.elapsed_time(e1) * 1e-3, 1e-6))))
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(reps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(reps)]
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)  # the sampler's first reading falls inside the timed region
+    for i in range(reps):
+        starts[i].record(stream)
+        execute()
+        ends[i].record(stream)
+        flush.zero_()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    lib.pd_plan_destroy(ctx.handle, plan)
+    ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends)) / reps
+    return {"value": w.pair_q / (ms * 1e-3), "unit": UNIT, "ms_per_solve": ms, "repeats": reps,
+            "n_atoms": req.n_atoms, "nq": req.nq, "n_frames": req.n_frames, "clocks": clk}
+
+
+def serving_burst(ctx, local, n_requests=400, precision="fp32"):
+    """n_requests requests of the serving stream's distribution submitted at
+    once to the request loop: p50/p99 latency and aggregate pair·q/s."""
+    from pripps_b200 import synth, workloads
+    from pripps_b200.serving import Server
+    stream = synth.request_stream(n_requests, 1e9, seed=4)
+    pool = workloads.GlobulePool()
+    reqs = [workloads.stream_request_pooled(sr, pool, precision) for sr in stream]
+    srv = Server(ctx)
+    for w in reqs[:3]:
+        srv.wait(srv.submit(w.request))
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    t0 = time.perf_counter()
+    tickets = [srv.submit(w.request) for w in reqs]
+    for t in tickets:
+        srv.wait(t)
+    wall = time.perf_counter() - t0
+    clk = clocks.stop()
+    lat = np.array([d - s for s, a, d in (srv.times(t) for t in tickets)])
+    pq = sum(w.pair_q for w in reqs)
+    return {"requests": n_requests, "arrival": "all at once", "value": pq / wall, "unit": UNIT,
+            "wall_s": wall, "latency_ms": {"p50": float(np.percentile(lat, 50) * 1e3),
+                                           "p99": float(np.percentile(lat, 99) * 1e3)},
+            "clocks": clk}
+
+
+def run_secondary(ctx, args, local):
+    """The other workloads, each timed for at least 2 s with its own clock
+    record, and a 400-request serving burst."""
+    from pripps_b200 import workloads
+    out = {}
+    for name in ("sphere_solvent_10k", "trajectory_5k_256"):
+        if name != args.workload:
+            out[name] = timed_workload(ctx, workloads.WORKLOADS[name](args.precision), local)
+    out["serving_burst_400"] = serving_burst(ctx, local, 400, args.precision)
+    return out
 
 
 def run_serve(args, ws, rank, local):
@@ -612,6 +719,8 @@ def main():
                     help="q points of the CPU baseline sample (0: two per host core)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-secondary", action="store_true",
+                    help="skip the other workloads and the serving burst")
     ap.add_argument("--serve", action="store_true", help="serving-stream benchmark")
     ap.add_argument("--direct", action="store_true", help="direct-transform benchmark")
     ap.add_argument("--p-max", type=int, default=100)

@@ -347,6 +347,29 @@ int result_status(pd_ctx *ctx, const Plan &P, int32_t status, const double *term
 }
 
 // Fill the pinned staging image (tables, layout, tiles, lists, descriptor).
+// Sizes of the request-derived regions of the staging image (tables,
+// weights, coordinates), which a re-staged plan copies unchanged.
+struct InputRegions {
+    uint64_t off[7];
+    uint64_t bytes[7];
+};
+InputRegions input_regions(const DevPlan &dp) {
+    const Plan &P = dp.P;
+    const Layout &L = dp.L;
+    const uint64_t tab = static_cast<uint64_t>(P.n_species) * P.nq * 8;
+    return InputRegions{
+        {L.qv, L.ffA, L.ffC, L.ffW, L.hw, L.fw, L.xyz},
+        {static_cast<uint64_t>(P.nq) * 8, tab, P.has_exc ? tab : 0,
+         P.has_hyd ? static_cast<uint64_t>(P.nq) * 8 : 0,
+         P.has_hyd ? static_cast<uint64_t>(P.n_atoms) * 8 : 0,
+         static_cast<uint64_t>(P.n_frames) * 8,
+         dp.host_xyz ? static_cast<uint64_t>(P.n_atoms) * 3 * P.n_frames * 8 : 0}};
+}
+
+// The plan-derived part of the staging image: classes, layout, tiles,
+// reduction lists, lattice descriptors and the request descriptor.
+void stage_structure(DevPlan &dp);
+
 int stage_plan(pd_ctx *ctx, DevPlan &dp, const pd_request *req) {
     const Plan &P = dp.P;
     const Layout &L = dp.L;
@@ -360,6 +383,17 @@ int stage_plan(pd_ctx *ctx, DevPlan &dp, const pd_request *req) {
     }
     double *fw = dp.hptr<double>(L.fw);
     for (int f = 0; f < P.n_frames; ++f) fw[f] = req->frame_weights ? req->frame_weights[f] : 1.0;
+    if (dp.host_xyz)
+        std::memcpy(dp.hptr<double>(L.xyz), req->xyz,
+                    static_cast<size_t>(P.n_atoms) * 3 * P.n_frames * 8);
+    stage_structure(dp);
+    (void)ctx;
+    return PD_OK;
+}
+
+void stage_structure(DevPlan &dp) {
+    const Plan &P = dp.P;
+    const Layout &L = dp.L;
     std::memcpy(dp.hptr<char>(L.cls), P.cls.data(), P.cls.size() * sizeof(PdClassDev));
     std::memcpy(dp.hptr<char>(L.pairs), P.pairs.data(), P.pairs.size() * sizeof(PdPairDev));
     std::memcpy(dp.hptr<char>(L.perm), P.perm.data(), P.perm.size() * 4);
@@ -392,11 +426,6 @@ int stage_plan(pd_ctx *ctx, DevPlan &dp, const pd_request *req) {
     std::memcpy(dp.hptr<char>(L.req), &rd, sizeof(rd));
     const int nj = static_cast<int>(P.jobs.size());
     std::memcpy(dp.hptr<char>(L.njobs), &nj, sizeof(int));
-    if (dp.host_xyz)
-        std::memcpy(dp.hptr<double>(L.xyz), req->xyz,
-                    static_cast<size_t>(P.n_atoms) * 3 * P.n_frames * 8);
-    (void)ctx;
-    return PD_OK;
 }
 
 constexpr int kBudgetWait = -100;  // internal: does not fit the budget right now
@@ -550,7 +579,7 @@ int run_devplan(pd_ctx *ctx, DevPlan &dp, double *out_dev, cudaStream_t st,
     // a streamed trajectory keeps the status of all its batches
     if (!dp.frame_sum) PD_CUDA(ctx, cudaMemsetAsync(dp.base + L.status, 0, 8, st));
     if (ev) cudaEventRecord(ev->first, st);
-    if (dp.world > 1)  // the lists also name the other ranks' slots
+    if (dp.world > 1)  // a frame's slot may be written by another rank's tile only
         PD_CUDA(ctx, cudaMemsetAsync(dp.dptr<double>(L.slots), 0,
                                      static_cast<size_t>(P.slots_per_frame) * P.n_frames * P.nv *
                                          P.tun.K * 8,
@@ -560,8 +589,7 @@ int run_devplan(pd_ctx *ctx, DevPlan &dp, double *out_dev, cudaStream_t st,
         PD_CUDA(ctx, pd::launch_pairs(P.precision, P.tun.K, P.tun.NP, P.mode, dp.dptr<PdJob>(L.jobs),
                                       dp.dptr<int>(L.njobs), dp.dptr<PdReqDev>(L.req),
                                       dp.dptr<int>(L.counter),
-                                      persistent_grid(ctx, P, static_cast<int64_t>(P.jobs.size()) /
-                                                                  static_cast<int64_t>(dp.world) + 1),
+                                      persistent_grid(ctx, P, static_cast<int64_t>(P.jobs.size())),
                                       st));
         ctx->launches += 1;
     }
@@ -574,6 +602,7 @@ int run_devplan(pd_ctx *ctx, DevPlan &dp, double *out_dev, cudaStream_t st,
 // ---------------------------------------------------------------- plan API
 struct pd_plan {
     DevPlan dp;
+    std::unique_ptr<Plan> full;  // the whole plan, kept once a shard replaces it
     bool profiling = false;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pair_events;  // one per execution
 };
@@ -1407,18 +1436,50 @@ int pd_plan_set_shard(pd_ctx *ctx, pd_plan *plan, uint32_t rank, uint32_t world)
     std::lock_guard<std::mutex> g(ctx->solve_mu);
     cudaSetDevice(ctx->device);
     DevPlan &dp = plan->dp;
-    // every world-th tile in execution (cost) order
-    std::vector<PdJob> mine;
-    mine.reserve(dp.P.jobs.size() / world + 1);
-    for (size_t t = rank; t < dp.P.jobs.size(); t += world) mine.push_back(dp.P.jobs[t]);
-    const int nj = static_cast<int>(mine.size());
-    PD_CUDA(ctx, cudaMemcpyAsync(dp.dptr<PdJob>(dp.L.jobs), mine.data(), mine.size() * sizeof(PdJob),
-                                 cudaMemcpyHostToDevice, ctx->stream));
-    PD_CUDA(ctx, cudaMemcpyAsync(dp.dptr<int>(dp.L.njobs), &nj, sizeof(int), cudaMemcpyHostToDevice,
-                                 ctx->stream));
-    PD_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-    dp.rank = rank;
-    dp.world = world;
+    if (!plan->full) plan->full = std::make_unique<Plan>(dp.P);
+    // A new device chunk holding only this rank's tiles, slots and lists;
+    // the request's tables are copied from the current staging image.
+    DevPlan nd;
+    pd::shard_plan(*plan->full, rank, world, nd.P);
+    nd.host_xyz = dp.host_xyz;
+    nd.frame_sum = dp.frame_sum;
+    nd.rank = rank;
+    nd.world = world;
+    nd.L = make_layout(nd.P, nd.host_xyz);
+    cudaStream_t st = ctx->stream;
+    // wait for executions of the old chunk first (they may be on caller streams)
+    PD_CUDA(ctx, cudaDeviceSynchronize());
+    const uint64_t need = nd.L.total;
+    const uint64_t have = dp.charged;
+    if (ctx->in_use.load() - have + need > ctx->budget) {
+        ctx->set_error("sharded plan does not fit the memory budget");
+        return PD_EBUDGET;
+    }
+    ctx->in_use.fetch_add(need);
+    nd.charged = need;
+    cudaError_t e = cudaMallocFromPoolAsync(reinterpret_cast<void **>(&nd.base), need, ctx->pool, st);
+    if (e == cudaSuccess) e = ctx->pinned.get(nd.L.stage_bytes, &nd.stage, &nd.stage_cls);
+    if (e != cudaSuccess) {
+        free_devplan(ctx, nd, st);
+        return cuda_fail(ctx, e, "pd_plan_set_shard");
+    }
+    const InputRegions from = input_regions(dp), to = input_regions(nd);
+    for (int r = 0; r < 7; ++r)
+        if (from.bytes[r]) std::memcpy(nd.stage + to.off[r], dp.stage + from.off[r], from.bytes[r]);
+    stage_structure(nd);
+    e = cudaMemcpyAsync(nd.base, nd.stage, nd.L.upload_bytes, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(nd.base + nd.L.status, 0, 8, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+        free_devplan(ctx, nd, st);
+        return cuda_fail(ctx, e, "pd_plan_set_shard");
+    }
+    free_devplan(ctx, dp, st);
+    cudaStreamSynchronize(st);
+    dp = std::move(nd);
+    nd.base = nullptr;
+    nd.stage = nullptr;
+    nd.charged = 0;
     return PD_OK;
 }
 

@@ -533,4 +533,48 @@ int build_plan(const pd_request *req, const uint32_t *species, const double *w,
     return PD_OK;
 }
 
+int shard_plan(const Plan &full, uint32_t rank, uint32_t world, Plan &out) {
+    out = full;
+    if (world <= 1) return PD_OK;
+    if (rank >= world) return PD_EINVAL;
+    const int64_t spf = full.slots_per_frame;
+    std::vector<int64_t> remap(static_cast<size_t>(spf), -1);
+    auto local_of = [&](const PdJob &jb) {
+        return (jb.slot & PD_SLOT_MASK) - static_cast<int64_t>(jb.frame) * spf;
+    };
+    auto nslot_of = [](const PdJob &jb) {
+        int n = 1;
+        for (int w = 0; w < PD_WARPS; ++w)
+            n = std::max(n, 1 + static_cast<int>((jb.slot >> (PD_SLOT_MAP_SHIFT + 2 * w)) & 3));
+        return n;
+    };
+    out.jobs.clear();
+    for (size_t t = rank; t < full.jobs.size(); t += world) {
+        const PdJob &jb = full.jobs[t];
+        const int64_t loc = local_of(jb);
+        for (int s = 0; s < nslot_of(jb); ++s) remap[static_cast<size_t>(loc + s)] = 0;
+        out.jobs.push_back(jb);
+    }
+    // this rank's slots, numbered in their original order (list order kept)
+    int64_t k = 0;
+    for (auto &r : remap)
+        if (r >= 0) r = k++;
+    out.slots_per_frame = k;
+    for (PdJob &jb : out.jobs) {
+        const int64_t loc = local_of(jb);
+        jb.slot = (jb.slot & ~PD_SLOT_MASK) |
+                  (static_cast<int64_t>(jb.frame) * k + remap[static_cast<size_t>(loc)]);
+    }
+    out.lidx.clear();
+    out.lptr.assign(full.lptr.size(), 0);
+    for (size_t e = 0; e + 1 < full.lptr.size(); ++e) {
+        for (int64_t x = full.lptr[e]; x < full.lptr[e + 1]; ++x) {
+            const int64_t r = remap[static_cast<size_t>(full.lidx[static_cast<size_t>(x)])];
+            if (r >= 0) out.lidx.push_back(r);
+        }
+        out.lptr[e + 1] = static_cast<int64_t>(out.lidx.size());
+    }
+    return PD_OK;
+}
+
 }  // namespace pd

@@ -74,6 +74,11 @@ int validate_request(const pd_request *req, bool device_pointers, std::string &m
 // Default shape when no tuned entry exists.
 Tuning default_tuning(int64_t n_atoms, int64_t nq, int precision, int64_t n_frames = 1);
 
+// A rank's share of a plan for a tile-sharded solve: every world-th tile of
+// the cost-ordered job list, with only the slots those tiles write (numbered
+// in their original order) and the reduction lists cut to them.
+int shard_plan(const Plan &full, uint32_t rank, uint32_t world, Plan &out);
+
 // Build the plan from host-side species and weights (hyd may be NULL).
 // count_pairs fills Plan::pairs_covered (an O(N · tiles per block) host loop
 // that only pd_plan_inspect needs).

@@ -72,3 +72,58 @@ def test_two_ranks_on_one_device_sum_to_the_single_rank_solve(tmp_path, gpu_ctx,
     got = np.load(path)
     ref = solve(_request(precision), gpu_ctx)
     assert np.all(term_errors(got, ref) < 1e-12), term_errors(got, ref)
+
+
+def _plan_info(plan):
+    import ctypes as C
+    from pripps_b200 import _lib
+    tiles, dbytes = C.c_uint64(), C.c_uint64()
+    _lib.check(_lib.lib().pd_plan_info(plan, None, None, None, C.byref(tiles), C.byref(dbytes),
+                                       None), None)
+    return tiles.value, dbytes.value
+
+
+def test_shard_plans_hold_only_their_share(gpu_ctx):
+    """A sharded plan keeps only its tiles' slots and lists: each of two
+    shards holds less device memory than the whole plan, their partial
+    profiles add up to the whole solve, and world = 1 restores the whole
+    plan bit for bit."""
+    import ctypes as C
+
+    import torch
+
+    from pripps_b200 import _lib
+    lib = _lib.lib()
+    req = _request("fp32")
+    r = req.c_struct()
+    xyz = torch.from_numpy(req.xyz).cuda()
+    sp = torch.cuda.current_stream().cuda_stream
+
+    def run(plan):
+        out = torch.empty((6, req.nq), dtype=torch.float64, device="cuda")
+        _lib.check(lib.pd_plan_execute(gpu_ctx.handle, plan, xyz.data_ptr(), out.data_ptr(), sp),
+                   gpu_ctx.handle)
+        torch.cuda.synchronize()
+        return out.cpu().numpy()
+
+    plans = []
+    try:
+        for _ in range(3):
+            p = C.c_void_p()
+            _lib.check(lib.pd_plan_create(gpu_ctx.handle, C.byref(r), C.byref(p)), gpu_ctx.handle)
+            plans.append(p)
+        whole = run(plans[2])
+        tiles_all, bytes_all = _plan_info(plans[2])
+        parts = []
+        for rank in range(2):
+            _lib.check(lib.pd_plan_set_shard(gpu_ctx.handle, plans[rank], rank, 2), gpu_ctx.handle)
+            tiles, nbytes = _plan_info(plans[rank])
+            assert tiles < tiles_all and nbytes < bytes_all
+            parts.append(run(plans[rank]))
+        assert np.all(term_errors(parts[0] + parts[1], whole) < 1e-12)
+        _lib.check(lib.pd_plan_set_shard(gpu_ctx.handle, plans[0], 0, 1), gpu_ctx.handle)
+        assert _plan_info(plans[0]) == (tiles_all, bytes_all)
+        assert np.array_equal(run(plans[0]), whole)
+    finally:
+        for p in plans:
+            lib.pd_plan_destroy(gpu_ctx.handle, p)
