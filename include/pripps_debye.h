@@ -300,6 +300,31 @@ int pd_wait(pd_ctx *ctx, uint64_t ticket, int timeout_ms, double *out_terms);
 int pd_poll(pd_ctx *ctx, uint64_t ticket);
 int pd_cancel(pd_ctx *ctx, uint64_t ticket);
 
+/* Serving replicas across GPUs: one request loop (context) per device in
+ * `devices` (the same ordinal may repeat: several loops share that GPU), and
+ * a router that sends each whole request to the replica with the least work
+ * still pending (pair·q × frames, FP64 counted 24×, the weighted mode 1.5×;
+ * ties go to the lowest index). Whole requests never split across replicas,
+ * so each result is the one its replica's loop gives alone. Tickets carry the
+ * replica in their top 8 bits. pd_router_wait / _poll / _cancel behave as
+ * pd_wait / pd_poll / pd_cancel on the replica; pd_router_replica names the
+ * replica and its context ticket (for pd_ticket_times); pd_route_choose is
+ * the routing policy itself (host-only): the index of the smallest pending
+ * work. Errors of router calls are described by pd_router_last_error().
+ * No reference counterpart (the reference is one process on one host). */
+typedef struct pd_router pd_router;
+int pd_router_create(const int *devices, uint32_t n_devices, uint64_t mem_budget_bytes,
+                     pd_router **out);
+void pd_router_destroy(pd_router *router);
+int pd_router_submit(pd_router *router, const pd_request *req, uint64_t *ticket);
+int pd_router_wait(pd_router *router, uint64_t ticket, int timeout_ms, double *out_terms);
+int pd_router_poll(pd_router *router, uint64_t ticket);
+int pd_router_cancel(pd_router *router, uint64_t ticket);
+int pd_router_replica(pd_router *router, uint64_t ticket, uint32_t *replica, pd_ctx **ctx,
+                      uint64_t *ctx_ticket);
+int pd_route_choose(const double *pending_work, uint32_t n, uint32_t *choice);
+const char *pd_router_last_error(void);
+
 /* Timestamps of a finished ticket in seconds on the context's monotonic
  * clock: submission, admission to the device, completion. */
 int pd_ticket_times(pd_ctx *ctx, uint64_t ticket, double *t_submit, double *t_admit,

@@ -133,6 +133,15 @@ SIGNATURES = {
     "pd_request_device_bytes": (C.c_int, [_P, C.POINTER(PdRequest), C.c_int, _U64P]),
     "pd_measure_fp32_peak": (C.c_int, [_P, _D, _D]),
     "pd_launch_count": (C.c_uint64, [_P]),
+    "pd_router_create": (C.c_int, [C.POINTER(C.c_int), C.c_uint32, C.c_uint64, C.POINTER(_P)]),
+    "pd_router_destroy": (None, [_P]),
+    "pd_router_submit": (C.c_int, [_P, C.POINTER(PdRequest), _U64P]),
+    "pd_router_wait": (C.c_int, [_P, C.c_uint64, C.c_int, _D]),
+    "pd_router_poll": (C.c_int, [_P, C.c_uint64]),
+    "pd_router_cancel": (C.c_int, [_P, C.c_uint64]),
+    "pd_router_replica": (C.c_int, [_P, C.c_uint64, _U32P, C.POINTER(_P), _U64P]),
+    "pd_route_choose": (C.c_int, [_D, C.c_uint32, _U32P]),
+    "pd_router_last_error": (C.c_char_p, []),
     "pd_solve_noalloc": (C.c_int, [C.POINTER(PdRequest), C.c_void_p, C.c_void_p, C.c_void_p]),
     "pd_direct": (C.c_int, [_P, C.POINTER(PdDirectRequest), _D]),
     "pd_direct_lattice": (C.c_int, [_P, C.POINTER(PdDirectRequest), C.POINTER(C.c_int32), _D,
