@@ -30,6 +30,7 @@
 #include "pripps_debye.h"
 
 #include <dlfcn.h>
+#include <nvtx3/nvToolsExt.h>
 
 using pd::Plan;
 using pd::Tuning;
@@ -46,6 +47,17 @@ double now_s() {
 }
 
 inline uint64_t align_up(uint64_t v, uint64_t a) { return (v + a - 1) / a * a; }
+
+// NVTX range over a host phase (planning, upload, the launches of each
+// kernel stage, the request loop's admission, steps and finishes), so that a
+// profiler timeline lines the host work up with the kernels it launched.
+// Without a profiler attached a range costs a few nanoseconds.
+struct NvtxRange {
+    explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange &) = delete;
+    NvtxRange &operator=(const NvtxRange &) = delete;
+};
 
 // Offsets of every array of one request inside its single device chunk. The
 // first `upload_bytes` bytes mirror a host staging image uploaded with one
@@ -433,6 +445,7 @@ constexpr int kBudgetWait = -100;  // internal: does not fit the budget right no
 // Host planning only: tiles, lists and the device layout.
 int plan_host(pd_ctx *ctx, const pd_request *req, const uint32_t *species, const double *weights,
               bool host_xyz, DevPlan &dp, const Tuning *force = nullptr) {
+    NvtxRange nvtx("pd plan (host)");
     std::string msg;
     const Tuning tun = force ? *force : tuning_for_request(ctx, req, species, weights);
     int rc = pd::build_plan(req, species, weights, tun, dp.P, msg);
@@ -454,6 +467,7 @@ int plan_host(pd_ctx *ctx, const pd_request *req, const uint32_t *species, const
 // upload. With `wait` a full budget returns kBudgetWait (retry after frees);
 // without it a full budget is PD_EBUDGET.
 int plan_device(pd_ctx *ctx, const pd_request *req, DevPlan &dp, cudaStream_t st, bool wait) {
+    NvtxRange nvtx("pd upload");
     const uint64_t need = dp.L.total;
     uint64_t cur = ctx->in_use.load();
     for (;;) {
@@ -499,6 +513,7 @@ int create_devplan(pd_ctx *ctx, const pd_request *req, const uint32_t *species,
 // Everything after the pair kernel: slot reduction, six-profile combine and
 // the frame mean; leaves the [6][nq] result at L.out (or out_dev).
 int finish_devplan(pd_ctx *ctx, DevPlan &dp, double *out_dev, cudaStream_t st) {
+    NvtxRange nvtx("pd reduce + combine");
     const Plan &P = dp.P;
     const Layout &L = dp.L;
     PD_CUDA(ctx, pd::launch_reduce(dp.dptr<double>(L.slots), dp.dptr<int64_t>(L.lptr),
@@ -537,6 +552,7 @@ int finish_devplan(pd_ctx *ctx, DevPlan &dp, double *out_dev, cudaStream_t st) {
 
 // centroid + pack of the coordinates into the padded class layout.
 int pack_devplan(pd_ctx *ctx, DevPlan &dp, cudaStream_t st) {
+    NvtxRange nvtx("pd pack");
     const Plan &P = dp.P;
     const Layout &L = dp.L;
     PD_CUDA(ctx, pd::launch_centroid(dp.xyz_dev, P.n_atoms, P.n_frames, dp.dptr<double>(L.centroid),
@@ -585,6 +601,7 @@ int run_devplan(pd_ctx *ctx, DevPlan &dp, double *out_dev, cudaStream_t st,
                                          P.tun.K * 8,
                                      st));
     if (!P.jobs.empty()) {
+        NvtxRange nvtx("pd pair kernel");
         PD_CUDA(ctx, cudaMemsetAsync(dp.dptr<int>(L.counter), 0, sizeof(int), st));
         PD_CUDA(ctx, pd::launch_pairs(P.precision, P.tun.K, P.tun.NP, P.mode, dp.dptr<PdJob>(L.jobs),
                                       dp.dptr<int>(L.njobs), dp.dptr<PdReqDev>(L.req),
@@ -837,6 +854,7 @@ void worker_main(pd_ctx *ctx) {
             if (head.empty()) std::this_thread::sleep_for(std::chrono::milliseconds(1));
             continue;
         }
+        nvtxRangePushA("pd admit");
         // ---- admission in FIFO order while the budget allows
         bool admitted_now = false;
         std::vector<std::shared_ptr<PdTicket>> fresh;  // admitted in this pass
@@ -880,6 +898,8 @@ void worker_main(pd_ctx *ctx) {
             admit_recorded = true;
         }
 
+        nvtxRangePop();
+        nvtxRangePushA("pd express + step");
         // ---- express: small requests admitted now get all their tiles on a
         // free express lane of their kernel variant (else they take the steps)
         {
@@ -1035,6 +1055,8 @@ void worker_main(pd_ctx *ctx) {
         if (n_lanes) cur = (cur + 1) % STEP_BUFS;
         (void)launch_failed;
 
+        nvtxRangePop();
+        nvtxRangePushA("pd finish + retire");
         // ---- finish requests whose tiles are all issued (or drain cancelled ones)
         for (auto &t : active) {
             if (t->status != 1 || t->finish_issued) continue;
@@ -1099,6 +1121,7 @@ void worker_main(pd_ctx *ctx) {
             it = remove ? active.erase(it) : it + 1;
         }
 
+        nvtxRangePop();
         // ---- nothing to issue: wait briefly for a submission or the GPU
         bool issuable = false;
         for (auto &t : active)
@@ -1256,6 +1279,7 @@ const char *pd_last_error(pd_ctx *ctx) {
 
 int pd_solve(pd_ctx *ctx, const pd_request *req, double *out_terms) {
     if (!ctx || !out_terms) return PD_EINVAL;
+    NvtxRange nvtx("pd_solve");
     std::string msg;
     int rc = pd::validate_request(req, false, msg);
     if (rc) {
@@ -1716,6 +1740,7 @@ std::vector<Tuning> tune_candidates(const pd_request *req, int mode) {
 // for the request's bucket. Each timed execution starts with L2 flushed (a
 // 256 MiB write), as a stream of independent requests would meet it.
 int autotune_request(pd_ctx *ctx, const pd_request *req, Tuning *best_out, double *best_ms) {
+    NvtxRange nvtx("pd autotune");
     std::string msg;
     int rc = pd::validate_request(req, false, msg);
     if (rc) {
