@@ -341,6 +341,14 @@ __device__ __forceinline__ void pairs_range(const float4 *__restrict__ at, int j
 // the grid end instead of computing and discarding them. (One uniform branch
 // per chunk in a single code path measured faster on B200 than a separate
 // copy of the loop for tail blocks, which raised register spills.)
+#ifndef PD_SCALED_V
+#define PD_SCALED_V 0
+#endif
+// Steps between two checks for the end of the grid (a chunk of 2·PD_CHUNK_T
+// grid points).
+#ifndef PD_CHUNK_T
+#define PD_CHUNK_T 8
+#endif
 template <int K, int NP, bool RESID, bool GENERAL_STEP>
 __device__ __forceinline__ void pairs_range_x2(const float4 *__restrict__ at, int jbase, float4 pi,
                                                int i, bool ivalid, int j0, int j1, float qs_hi,
@@ -353,14 +361,24 @@ __device__ __forceinline__ void pairs_range_x2(const float4 *__restrict__ at, in
     SeedGroup<PD_MODE_CLASS, NP, RESID, GENERAL_STEP> cur;
     cur.make(at, jbase, pi, i, ivalid, j0, j1, qs_hi, qs_lo, dq_hi, dq_lo);
     for (int j = j0; j < j1; j += NP) {
+        // SCALED: without the general step every term of a pair has the
+        // weight w = 1/r, which the linear recurrence can carry in v and d
+        // themselves; the accumulation is then a plain add.
+        constexpr bool SCALED = PD_SCALED_V && !GENERAL_STEP;
         float2 V[NP], D[NP], NA[NP], WE[NP], WO[NP];
 #pragma unroll
         for (int p = 0; p < NP; ++p) {
-            V[p] = make_float2(cur.S[p].ve, cur.S[p].vo);
-            D[p] = make_float2(cur.S[p].de, cur.S[p].dd);
+            if (SCALED) {
+                const float w = cur.S[p].we;
+                V[p] = make_float2(w * cur.S[p].ve, w * cur.S[p].vo);
+                D[p] = make_float2(w * cur.S[p].de, w * cur.S[p].dd);
+            } else {
+                V[p] = make_float2(cur.S[p].ve, cur.S[p].vo);
+                D[p] = make_float2(cur.S[p].de, cur.S[p].dd);
+                WE[p] = make_float2(cur.S[p].we, cur.S[p].we);
+                WO[p] = GENERAL_STEP ? make_float2(cur.S[p].wo, cur.S[p].wo) : WE[p];
+            }
             NA[p] = make_float2(cur.S[p].na, cur.S[p].na);
-            WE[p] = make_float2(cur.S[p].we, cur.S[p].we);
-            WO[p] = GENERAL_STEP ? make_float2(cur.S[p].wo, cur.S[p].wo) : WE[p];
         }
         const float2 mvs = make_float2(-cur.vsum, -cur.vsum);
         // the next pass's seeds (unused after the last pass), computed in
@@ -370,7 +388,7 @@ __device__ __forceinline__ void pairs_range_x2(const float4 *__restrict__ at, in
         if (RESID) asm volatile("mov.b32 %0, %0;" : "+r"(qoff));
 #pragma unroll
         for (int t = 0; t < K / 2; ++t) {
-            if ((t % 8) == 0 && t / 8 >= nchunk) break;
+            if ((t % PD_CHUNK_T) == 0 && t / PD_CHUNK_T >= nchunk) break;
             // the residual points are a prefix of the block: only its first
             // rchunk 16-point chunks subtract q
             if (RESID && (t / 8) < rchunk) acc[t] = __ffma2_rn(mvs, s_qres2[t + qoff], acc[t]);
@@ -380,8 +398,12 @@ __device__ __forceinline__ void pairs_range_x2(const float4 *__restrict__ at, in
 #pragma unroll
             for (int p = 0; p < NP; ++p) D[p] = __ffma2_rn(NA[p], V[p], D[p]);
 #pragma unroll
-            for (int p = 0; p < NP; ++p)
-                acc[t] = __ffma2_rn((t & 1) ? WO[p] : WE[p], V[p], acc[t]);
+            for (int p = 0; p < NP; ++p) {
+                if constexpr (SCALED)
+                    acc[t] = __fadd2_rn(V[p], acc[t]);
+                else
+                    acc[t] = __ffma2_rn((t & 1) ? WO[p] : WE[p], V[p], acc[t]);
+            }
 #pragma unroll
             for (int p = 0; p < NP; ++p) V[p] = __fadd2_rn(V[p], D[p]);
         }
@@ -555,7 +577,8 @@ __global__ void __launch_bounds__(PD_THREADS, fp32_min_blocks(K, MODE, NP))
                         // The small-q residual blocks (the first of a grid)
                         // run whole: a tail check there costs the register
                         // spills it saves in steps.
-                        const int nchunk = (min(K, rq.nq - kq0) + 15) >> 4;
+                        const int nchunk =
+                            (min(K, rq.nq - kq0) + 2 * PD_CHUNK_T - 1) / (2 * PD_CHUNK_T);
                         float2 acc[K / 2];
 #pragma unroll
                         for (int t = 0; t < K / 2; ++t) acc[t] = make_float2(0.0f, 0.0f);
@@ -563,11 +586,12 @@ __global__ void __launch_bounds__(PD_THREADS, fp32_min_blocks(K, MODE, NP))
                             if (general_step)
                                 pairs_range_x2<K, NP, true, true>(chunk, jss, pi, i, ivalid, js, je,
                                                                   qs_hi, qs_lo, dq_hi, dq_lo, q2,
-                                                                  acc, K / 16, rchunk);
+                                                                  acc, K / (2 * PD_CHUNK_T), rchunk);
                             else
                                 pairs_range_x2<K, NP, true, false>(chunk, jss, pi, i, ivalid, js,
                                                                    je, qs_hi, qs_lo, dq_hi, dq_lo,
-                                                                   q2, acc, K / 16, rchunk);
+                                                                   q2, acc, K / (2 * PD_CHUNK_T),
+                                                                   rchunk);
                         } else {
                             if (general_step)
                                 pairs_range_x2<K, NP, false, true>(chunk, jss, pi, i, ivalid, js,
