@@ -344,6 +344,11 @@ __device__ __forceinline__ void pairs_range(const float4 *__restrict__ at, int j
 #ifndef PD_SCALED_V
 #define PD_SCALED_V 0
 #endif
+// Instruction order within a step: 0 = d-steps, accumulations, v-steps;
+// 1 = d-steps, then per pair its accumulation and v-step.
+#ifndef PD_STEP_ORDER
+#define PD_STEP_ORDER 0
+#endif
 // Steps between two checks for the end of the grid (a chunk of 2·PD_CHUNK_T
 // grid points).
 #ifndef PD_CHUNK_T
@@ -397,15 +402,27 @@ __device__ __forceinline__ void pairs_range_x2(const float4 *__restrict__ at, in
             // (measured 0.5 % faster than the per-pair order).
 #pragma unroll
             for (int p = 0; p < NP; ++p) D[p] = __ffma2_rn(NA[p], V[p], D[p]);
+            if constexpr (PD_STEP_ORDER == 0) {
 #pragma unroll
-            for (int p = 0; p < NP; ++p) {
-                if constexpr (SCALED)
-                    acc[t] = __fadd2_rn(V[p], acc[t]);
-                else
-                    acc[t] = __ffma2_rn((t & 1) ? WO[p] : WE[p], V[p], acc[t]);
+                for (int p = 0; p < NP; ++p) {
+                    if constexpr (SCALED)
+                        acc[t] = __fadd2_rn(V[p], acc[t]);
+                    else
+                        acc[t] = __ffma2_rn((t & 1) ? WO[p] : WE[p], V[p], acc[t]);
+                }
+#pragma unroll
+                for (int p = 0; p < NP; ++p) V[p] = __fadd2_rn(V[p], D[p]);
+            } else {
+                // each pair's accumulation, then its v-step
+#pragma unroll
+                for (int p = 0; p < NP; ++p) {
+                    if constexpr (SCALED)
+                        acc[t] = __fadd2_rn(V[p], acc[t]);
+                    else
+                        acc[t] = __ffma2_rn((t & 1) ? WO[p] : WE[p], V[p], acc[t]);
+                    V[p] = __fadd2_rn(V[p], D[p]);
+                }
             }
-#pragma unroll
-            for (int p = 0; p < NP; ++p) V[p] = __fadd2_rn(V[p], D[p]);
         }
     }
 }
