@@ -501,6 +501,13 @@ __global__ void __launch_bounds__(PD_THREADS, fp32_min_blocks(K, MODE, NP))
     extern __shared__ __align__(128) float4 pd_dyn_atoms[];
     float4 *s_atoms[2] = {pd_dyn_atoms, pd_dyn_atoms + PD_JSTAGE};
     __shared__ __align__(8) unsigned long long s_bar[2];
+    // Once a copy wait of this CTA expires the CTA is "dead" for the rest of
+    // the launch: it issues no more copies, computes nothing, writes NaN to
+    // the slots of every tile it still takes and flags each tile's request
+    // in its status word. This state lives in shared memory, not registers,
+    // so that it adds nothing to the register pressure of the steps.
+    __shared__ int s_dead, s_first, s_polls, s_skip;
+    __shared__ uint32_t s_inflight, s_par;  // thread 0: copies in flight, their parities
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const int n_jobs = *n_jobs_ptr;
@@ -508,15 +515,11 @@ __global__ void __launch_bounds__(PD_THREADS, fp32_min_blocks(K, MODE, NP))
         mbar_init(&s_bar[0], 1);
         mbar_init(&s_bar[1], 1);
         mbar_init_fence();
+        s_dead = 0;
+        s_first = 1;
     }
     __syncthreads();
     uint32_t phase = 0;  // bit b: parity of buffer b's next completion
-    // Once a copy wait of this CTA expires the CTA is "dead" for the rest of
-    // the launch: it issues no more copies, computes nothing, writes NaN to
-    // the slots of every tile it still takes and flags each tile's request
-    // in its status word. (Uniform across the CTA.)
-    bool dead = false;
-    bool first_tile = true;
     double *part = s_part + warp * NV * K;
     for (;;) {
         if (threadIdx.x == 0) s_job = atomicAdd(counter, 1);
@@ -542,7 +545,17 @@ __global__ void __launch_bounds__(PD_THREADS, fp32_min_blocks(K, MODE, NP))
             }
         }
         const int rchunk = (nres + 15) >> 4;
-        __syncthreads();  // s_qres ready; every thread has read s_job
+        if (threadIdx.x == 0) {
+            // test hook: the first tile of CTA 0 waits for a copy that is
+            // never issued, briefly, so that its wait expires with no copy in
+            // flight
+            s_skip = (rq.flags & PD_REQF_TEST_EXPIRE) != 0 && blockIdx.x == 0 && s_first;
+            s_polls = s_skip ? PD_TEST_WAIT_POLLS : PD_WAIT_POLLS;
+            s_first = 0;
+            s_inflight = 0;
+            s_par = 0;
+        }
+        __syncthreads();  // s_qres and the tile state ready; every thread has read s_job
         const float4 *__restrict__ at = rq.atoms32 + static_cast<size_t>(jb.frame) * rq.n_pad;
         const int i = jb.i0 + threadIdx.x;
         const float4 pi = at[i];
@@ -555,36 +568,34 @@ __global__ void __launch_bounds__(PD_THREADS, fp32_min_blocks(K, MODE, NP))
         // Every pair distance is at most 2·radius (positions are centred):
         // below π/4 for the step angle Δq·r the seeds skip its reduction.
         const bool general_step = rq.dq * (2.0 * radius) > 0.78;
-        const int nstage = dead ? 0 : (jb.j1 - jb.j0 + PD_JSTAGE - 1) / PD_JSTAGE;
-        // test hook: the first tile of CTA 0 waits for a copy that is never
-        // issued, briefly, so that its wait expires with no copy in flight
-        const bool test_skip =
-            (rq.flags & PD_REQF_TEST_EXPIRE) != 0 && blockIdx.x == 0 && first_tile;
-        first_tile = false;
-        const int polls = test_skip ? PD_TEST_WAIT_POLLS : PD_WAIT_POLLS;
-        // thread 0: buffers with a copy in flight, and the parity of each
-        uint32_t inflight = 0, par = 0;
-        auto issue = [&](int b, int j_from, int j_to) {
-            bulk_copy_to_shared(s_atoms[b], at + j_from, static_cast<uint32_t>(j_to - j_from) * 16,
-                                &s_bar[b]);
-            inflight |= 1u << b;
-            par = (par & ~(1u << b)) | (phase & (1u << b));
-        };
-        if (threadIdx.x == 0 && nstage > 0 && !test_skip)
-            issue(0, jb.j0, min(jb.j1, jb.j0 + PD_JSTAGE));
+        const int nstage = s_dead ? 0 : (jb.j1 - jb.j0 + PD_JSTAGE - 1) / PD_JSTAGE;
+        if (threadIdx.x == 0 && nstage > 0 && !s_skip) {
+            bulk_copy_to_shared(s_atoms[0], at + jb.j0,
+                                static_cast<uint32_t>(min(jb.j1 - jb.j0, PD_JSTAGE)) * 16,
+                                &s_bar[0]);
+            s_inflight = 1u;
+            s_par = phase & 1u;
+        }
         for (int stg = 0; stg < nstage; ++stg) {
             const int jss = jb.j0 + stg * PD_JSTAGE;
             const int jse = min(jb.j1, jss + PD_JSTAGE);
-            if (threadIdx.x == 0 && stg + 1 < nstage)  // its buffer was released at stg - 1
-                issue((stg + 1) & 1, jse, min(jb.j1, jse + PD_JSTAGE));
+            if (threadIdx.x == 0 && stg + 1 < nstage) {  // its buffer was released at stg - 1
+                const int nb = (stg + 1) & 1;
+                bulk_copy_to_shared(s_atoms[nb], at + jse,
+                                    static_cast<uint32_t>(min(jb.j1 - jse, PD_JSTAGE)) * 16,
+                                    &s_bar[nb]);
+                s_inflight |= 1u << nb;
+                s_par = (s_par & ~(1u << nb)) | (phase & (1u << nb));
+            }
             const int b = stg & 1;
-            const bool got = mbar_wait(&s_bar[b], (phase >> b) & 1u, polls);
+            const bool landed = mbar_wait(&s_bar[b], (phase >> b) & 1u, s_polls);
             phase ^= 1u << b;
-            if (threadIdx.x == 0 && got) inflight &= ~(1u << b);
-            // the compute below has warp collectives: decide per warp
-            const bool landed = __all_sync(0xffffffffu, got);
+            if (threadIdx.x == 0 && landed) s_inflight &= ~(1u << b);
+            // A chunk that did not land is computed anyway (its shared memory
+            // holds stale atoms, harmless to read) and the tile is poisoned
+            // below: no branch around the steps.
             const float4 *chunk = s_atoms[b];
-            if (landed) {
+            {
                 for (int js = jss; js < jse; js += PD_JFLUSH) {
                     const int je = min(jse, js + PD_JFLUSH);
                     const bool first = js == jb.j0;
@@ -677,22 +688,34 @@ __global__ void __launch_bounds__(PD_THREADS, fp32_min_blocks(K, MODE, NP))
                 }
             }
             // every read of buffer b done before it is refilled; an expired
-            // wait in any warp makes the whole CTA dead
+            // wait in any thread makes the whole CTA dead
             if (__syncthreads_or(!landed)) {
-                dead = true;
+                if (threadIdx.x == 0) s_dead = 1;
                 break;
             }
         }
-        if (dead && threadIdx.x == 0) {
-            // no copy of this CTA may land in shared memory after it moves
-            // on: wait (bounded) for the ones still in flight
-            for (int b = 0; b < 2; ++b)
-                if (inflight & (1u << b)) mbar_wait(&s_bar[b], (par >> b) & 1u, PD_WAIT_POLLS);
-            atomicOr(rq.status, PD_DEV_WAIT_EXPIRED);
+        __syncthreads();  // every warp's partial sums are complete; s_dead final
+        {
+            // The job and request fields of the epilogue are loaded again here
+            // (an opaque index keeps the compiler from holding them in
+            // registers through the steps).
+            int jid2 = s_job;
+            asm volatile("" : "+r"(jid2));
+            const int64_t slot_word = jobs[jid2].slot;
+            const PdReqDev *rq2 = reqs + jobs[jid2].req;
+            const bool dead = s_dead != 0;
+            if (dead && threadIdx.x == 0) {
+                // no copy of this CTA may land in shared memory after it
+                // moves on: wait (bounded) for the ones still in flight
+                for (int b = 0; b < 2; ++b)
+                    if (s_inflight & (1u << b))
+                        mbar_wait(&s_bar[b], (s_par >> b) & 1u, PD_WAIT_POLLS);
+                atomicOr(rq2->status, PD_DEV_WAIT_EXPIRED);
+            }
+            merge_tile_slots(s_part, NV * K, slot_word, rq2->slots, dead,
+                             jobs[jid2].j1 <= jobs[jid2].j0 && !dead);
         }
-        __syncthreads();  // every warp's partial sums are complete
-        merge_tile_slots(s_part, NV * K, jb.slot, rq.slots, dead, nstage == 0 && !dead);
-        __syncthreads();  // s_qres, s_part and s_job are rewritten by the next tile
+        __syncthreads();  // s_qres, s_part, s_job and the tile state are rewritten next
     }
 }
 

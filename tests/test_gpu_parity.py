@@ -343,15 +343,16 @@ def test_serving_budget_admission(gpu_ctx):
     PD_EBUDGET."""
     from pripps_b200.errors import DeviceError
     from pripps_b200.serving import Server
+    # each request holds about 1.2 MB of device memory (pd_request_device_bytes)
     reqs = [workloads.small_globule(4000, s, nq=200).request for s in range(3)]
-    ctx = _lib.Context(0, mem_budget_bytes=64 << 20)
+    ctx = _lib.Context(0, mem_budget_bytes=2 << 20)
     try:
         srv = Server(ctx)
         solo = [solve(r, gpu_ctx) for r in reqs]
         ts = [srv.submit(r) for r in reqs]
         for t, ref in zip(ts, solo):
             assert np.array_equal(srv.wait(t, timeout_s=120), ref)
-        big = workloads.small_globule(60_000, 1, nq=900).request
+        big = workloads.small_globule(20_000, 1, nq=900).request  # about 11 MB
         t = srv.submit(big)
         with pytest.raises(DeviceError):
             srv.wait(t, timeout_s=120)
