@@ -68,13 +68,27 @@ def lookup(req, ctx=None):
     return (k.value, tj.value, np_.value), bool(tab.value)
 
 
-def test_lookup_without_context_is_the_default_shape():
-    if SHIPPED.exists() or os.environ.get("PRIPPS_DEBYE_TUNING"):
-        pytest.skip("a tuning table is installed")
-    shape, from_table = lookup(workloads.small_globule(5000, 1, nq=300).request)
-    # q block 128 with two pairs per thread from 4,000 atoms up; the j chunk
-    # is halved until a solve has about six tiles per resident CTA
-    assert not from_table and shape == (128, 256, 2)
+def test_lookup_without_context_uses_the_shipped_table():
+    """Without a context the lookup uses the table a new context would load:
+    the shipped file's entry for a tuned bucket, the default shape for a
+    bucket the file does not name."""
+    if os.environ.get("PRIPPS_DEBYE_TUNING") or not SHIPPED.exists():
+        pytest.skip("no shipped table in use")
+    entries = {}
+    for line in SHIPPED.read_text().splitlines():
+        f = line.split("#")[0].split()
+        if f:
+            entries[tuple(f[:5])] = (int(f[5]), int(f[6]), int(f[7]))
+    w = workloads.small_globule(5000, 1, nq=300)  # 2^12 <= 5,000 < 2^13, 2^8 <= 300 < 2^9
+    key = ("fp32", "class", "single", "12", "8")
+    shape, from_table = lookup(w.request)
+    assert from_table == (key in entries)
+    if from_table:
+        assert shape == entries[key]
+    w64 = workloads.small_globule(5000, 1, nq=300, precision="fp64")
+    if ("fp64", "class", "single", "12", "8") not in entries:
+        shape64, tab64 = lookup(w64.request)
+        assert not tab64 and shape64[2] == 1
 
 
 @pytest.mark.gpu
