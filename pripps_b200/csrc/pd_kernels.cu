@@ -39,6 +39,37 @@ __device__ __forceinline__ float warp_sum(float v) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     return v;
 }
+// Reduce-scatter of 2·NT values per lane (NT packed pairs, NT a multiple of
+// 32) over a warp: at each of five levels a lane keeps one half of its
+// pairs, sends the other half to its partner lane^o and adds what the
+// partner sends for the half it keeps. Afterwards lane l holds the warp sums
+// of the values [l·2NT/32, (l+1)·2NT/32) in v[0 .. NT/32). About 2·NT
+// shuffles and NT packed additions instead of the 10·NT shuffles and
+// additions of one butterfly per value; the order of the additions is fixed,
+// so the sums are deterministic.
+#ifndef PD_FLUSH_RS
+#define PD_FLUSH_RS 1
+#endif
+template <int NT>
+__device__ __forceinline__ void warp_reduce_scatter(float2 (&v)[NT], int lane) {
+    static_assert(NT % 32 == 0, "2·NT values must split evenly over 32 lanes in pairs");
+#pragma unroll
+    for (int lev = 0; lev < 5; ++lev) {
+        const int o = 16 >> lev;
+        const int h = (NT >> lev) / 2;  // packed pairs kept
+        const bool up = (lane & o) != 0;
+#pragma unroll
+        for (int k = 0; k < h; ++k) {
+            const float2 lo = v[k], hi = v[k + h];
+            const float2 keep = up ? hi : lo;
+            const float2 send = up ? lo : hi;
+            const float2 got = make_float2(__shfl_xor_sync(0xffffffffu, send.x, o),
+                                           __shfl_xor_sync(0xffffffffu, send.y, o));
+            v[k] = __fadd2_rn(keep, got);
+        }
+    }
+}
+
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -180,6 +211,118 @@ __device__ __forceinline__ PairSeed pair_seed(float4 pi, float4 pj, bool valid, 
     return ps;
 }
 
+// The seeds of two pairs at once on packed FP32x2 instructions: every
+// operation of pair_seed, in the same order and with the same roundings (a
+// negation is a multiplication by -1, exact), with pair 0 in the low and
+// pair 1 in the high half. Half the issue slots of two scalar seeds, and the
+// packed operations occupy both FP32 sub-pipes together instead of leaving
+// one of them idle beside a scalar operation.
+#ifndef PD_SEED_X2
+#define PD_SEED_X2 1
+#endif
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ void sincos_poly_x2(float2 t, float2 &s, float2 &c) {
+    const float2 t2 = __fmul2_rn(t, t);
+    float2 ps = f2(2.789128530e-6f);
+    ps = __ffma2_rn(ps, t2, f2(-1.984876289e-4f));
+    ps = __ffma2_rn(ps, t2, f2(8.333369158e-3f));
+    ps = __ffma2_rn(ps, t2, f2(-1.666666716e-1f));
+    s = __ffma2_rn(__fmul2_rn(t, t2), ps, t);
+    float2 pc = f2(2.443297126e-5f);
+    pc = __ffma2_rn(pc, t2, f2(-1.388731296e-3f));
+    pc = __ffma2_rn(pc, t2, f2(4.166664556e-2f));
+    pc = __ffma2_rn(pc, t2, f2(-0.5f));
+    c = __ffma2_rn(t2, pc, f2(1.0f));
+}
+// reduce_pio2 on both halves; the quadrants come back as integers.
+__device__ __forceinline__ float2 reduce_pio2_x2(float2 a_hi, float2 a_lo, int &q0, int &q1) {
+    const float2 nm = __ffma2_rn(a_hi, f2(0.636619772f), f2(kRoundMagic));
+    const float2 n = __fadd2_rn(nm, f2(-kRoundMagic));  // exact
+    q0 = __float_as_int(nm.x) & 3;
+    q1 = __float_as_int(nm.y) & 3;
+    const float2 t1 = __ffma2_rn(n, f2(-kPio2C1), a_hi);
+    return __fadd2_rn(t1, __ffma2_rn(n, f2(-kPio2C2), a_lo));
+}
+
+template <bool GENERAL_STEP>
+__device__ __forceinline__ void pair_seed_x2(float4 pi, float4 pj0, float4 pj1, bool valid0,
+                                             bool valid1, float qs_hi, float qs_lo, float dq_hi,
+                                             float dq_lo, PairSeed &S0, PairSeed &S1) {
+    const float2 M1 = f2(-1.0f);
+    const float2 dx = __ffma2_rn(make_float2(pj0.x, pj1.x), M1, f2(pi.x));
+    const float2 dy = __ffma2_rn(make_float2(pj0.y, pj1.y), M1, f2(pi.y));
+    const float2 dz = __ffma2_rn(make_float2(pj0.z, pj1.z), M1, f2(pi.z));
+    float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+    r2 = make_float2(fmaxf(r2.x, 1e-12f), fmaxf(r2.y, 1e-12f));
+    float2 inv_r = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+    const float2 r_hi = __fmul2_rn(r2, inv_r);
+    const float2 nr_hi = __fmul2_rn(r_hi, M1);
+    const float2 hinv = __fmul2_rn(f2(0.5f), inv_r);
+    const float2 r_lo = __fmul2_rn(hinv, __ffma2_rn(nr_hi, r_hi, r2));
+    inv_r = __ffma2_rn(hinv, __ffma2_rn(nr_hi, inv_r, f2(1.0f)), inv_r);
+    const float2 th_hi = __fmul2_rn(f2(qs_hi), r_hi);
+    const float2 th_lo =
+        __ffma2_rn(f2(qs_lo), r_hi,
+                   __ffma2_rn(f2(qs_hi), r_lo,
+                              __ffma2_rn(f2(qs_hi), r_hi, __fmul2_rn(th_hi, M1))));
+    int qt0, qt1;
+    const float2 t = reduce_pio2_x2(th_hi, th_lo, qt0, qt1);
+    float2 st, ct;
+    sincos_poly_x2(t, st, ct);
+    float s0a, c0a, s0b, c0b;
+    apply_quadrant(qt0, st.x, ct.x, s0a, c0a);
+    apply_quadrant(qt1, st.y, ct.y, s0b, c0b);
+    const float2 s0 = make_float2(s0a, s0b), c0 = make_float2(c0a, c0b);
+    const float w0 = valid0 ? inv_r.x : 0.0f, w1 = valid1 ? inv_r.y : 0.0f;
+    S0.ve = s0a;
+    S1.ve = s0b;
+    if (!GENERAL_STEP) {
+        const float2 x = __ffma2_rn(f2(dq_hi), r_hi,
+                                    __ffma2_rn(f2(dq_hi), r_lo, __fmul2_rn(f2(dq_lo), r_hi)));
+        float2 sx, cx;
+        sincos_poly_x2(x, sx, cx);
+        const float2 sx2 = __fmul2_rn(f2(2.0f), sx);
+        const float2 de = __fmul2_rn(sx2, __ffma2_rn(c0, cx, __fmul2_rn(s0, sx)));
+        const float2 vo = __ffma2_rn(s0, cx, __fmul2_rn(c0, sx));
+        const float2 dd = __fmul2_rn(sx2, c0);
+        const float2 na = __fmul2_rn(__fmul2_rn(sx2, M1), sx2);
+        S0.de = de.x; S1.de = de.y;
+        S0.vo = vo.x; S1.vo = vo.y;
+        S0.dd = dd.x; S1.dd = dd.y;
+        S0.na = na.x; S1.na = na.y;
+        S0.we = S0.wo = w0;
+        S1.we = S1.wo = w1;
+    } else {
+        const float2 x_hi = __fmul2_rn(f2(dq_hi), r_hi);
+        const float2 x_lo =
+            __ffma2_rn(f2(dq_lo), r_hi,
+                       __ffma2_rn(f2(dq_hi), r_lo,
+                                  __ffma2_rn(f2(dq_hi), r_hi, __fmul2_rn(x_hi, M1))));
+        int qm0, qm1;
+        const float2 h = reduce_pio2_x2(x_hi, x_lo, qm0, qm1);
+        float2 sh, ch;
+        sincos_poly_x2(h, sh, ch);
+        float sxa, cxa, sxb, cxb;
+        apply_quadrant(qm0, sh.x, ch.x, sxa, cxa);
+        apply_quadrant(qm1, sh.y, ch.y, sxb, cxb);
+        const float2 sx = make_float2(sxa, sxb), cx = make_float2(cxa, cxb);
+        const float2 s1 = __ffma2_rn(s0, cx, __fmul2_rn(c0, sx));
+        const float2 c1 = __ffma2_rn(c0, cx, __fmul2_rn(__fmul2_rn(s0, M1), sx));
+        const float2 sh2 = __fmul2_rn(f2(2.0f), sh);
+        const float2 de = __fmul2_rn(sh2, __ffma2_rn(c0, ch, __fmul2_rn(s0, sh)));
+        const float2 dd = __fmul2_rn(sh2, __ffma2_rn(c1, ch, __fmul2_rn(s1, sh)));
+        const float2 na = __fmul2_rn(__fmul2_rn(sh2, M1), sh2);
+        S0.de = de.x; S1.de = de.y;
+        S0.vo = s1.x; S1.vo = s1.y;
+        S0.dd = dd.x; S1.dd = dd.y;
+        S0.na = na.x; S1.na = na.y;
+        S0.we = w0;
+        S1.we = w1;
+        S0.wo = (qm0 & 1) ? -w0 : w0;
+        S1.wo = (qm1 & 1) ? -w1 : w1;
+    }
+}
+
 // Small-q residual form: where q·(2·radius) < 2 every pair has q·r < 2 and
 // the terms sin(q r)/r lie within a factor 0.45..1 of q, so a sequential FP32
 // sum of them rounds with a systematic bias. There the kernel accumulates
@@ -249,6 +392,20 @@ struct SeedGroup {
                                          float qs_lo, float dq_hi, float dq_lo) {
         vsum = 0.0f;
         vwsum = 0.0f;
+        if constexpr (PD_SEED_X2 && MODE == PD_MODE_CLASS && NP % 2 == 0) {
+#pragma unroll
+            for (int p = 0; p < NP; p += 2) {
+                const int ja = j + p, jb = j + p + 1;
+                const bool ina = ja < j1, inb = jb < j1;
+                const float4 pja = at[(ina ? ja : j1 - 1) - jbase];
+                const float4 pjb = at[(inb ? jb : j1 - 1) - jbase];
+                const bool va = ivalid && ina && (ja > i), vb = ivalid && inb && (jb > i);
+                pair_seed_x2<GENERAL_STEP>(pi, pja, pjb, va, vb, qs_hi, qs_lo, dq_hi, dq_lo,
+                                           S[p], S[p + 1]);
+                if (RESID) vsum += (va ? 1.0f : 0.0f) + (vb ? 1.0f : 0.0f);
+            }
+            return;
+        }
 #pragma unroll
         for (int p = 0; p < NP; ++p) {
             const int jj = j + p;
@@ -632,6 +789,17 @@ __global__ void __launch_bounds__(PD_THREADS, fp32_min_blocks(K, MODE, NP))
                         }
                         // Warp-reduce and add into this warp's partial sums,
                         // in sub-chunk order (one warp owns them).
+                        if constexpr (PD_FLUSH_RS && (K / 2) % 32 == 0) {
+                        // reduce-scatter: lane l ends with the warp sums of
+                        // grid points [l·K/32, (l+1)·K/32)
+                        warp_reduce_scatter<K / 2>(acc, lane);
+#pragma unroll
+                        for (int m = 0; m < K / 32; ++m) {
+                            double &d = part[lane * (K / 32) + m];
+                            const float sum = (m & 1) ? acc[m >> 1].y : acc[m >> 1].x;
+                            d = (first ? 0.0 : d) + static_cast<double>(sum);
+                        }
+                        } else {
 #pragma unroll
                         for (int t = 0; t < K / 2; ++t) {
                             const float v0 = warp_sum(acc[t].x);
@@ -641,6 +809,7 @@ __global__ void __launch_bounds__(PD_THREADS, fp32_min_blocks(K, MODE, NP))
                             if (lane == ((2 * t + 1) & 31))
                                 part[2 * t + 1] =
                                     (first ? 0.0 : part[2 * t + 1]) + static_cast<double>(v1);
+                        }
                         }
                     } else {
                         const float wi = ivalid ? pi.w : 0.0f;
