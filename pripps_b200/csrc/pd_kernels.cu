@@ -502,7 +502,9 @@ __device__ __forceinline__ void pairs_range(const float4 *__restrict__ at, int j
 #define PD_SCALED_V 0
 #endif
 // Instruction order within a step: 0 = d-steps, accumulations, v-steps;
-// 1 = d-steps, then per pair its accumulation and v-step.
+// 1 = d-steps, then per pair its accumulation and v-step; 2 (with
+// PD_SCALED_V, two pairs) = the two scaled terms summed, then added to the
+// accumulator.
 #ifndef PD_STEP_ORDER
 #define PD_STEP_ORDER 0
 #endif
@@ -559,7 +561,14 @@ __device__ __forceinline__ void pairs_range_x2(const float4 *__restrict__ at, in
             // (measured 0.5 % faster than the per-pair order).
 #pragma unroll
             for (int p = 0; p < NP; ++p) D[p] = __ffma2_rn(NA[p], V[p], D[p]);
-            if constexpr (PD_STEP_ORDER == 0) {
+            if constexpr (SCALED && PD_STEP_ORDER == 2 && NP == 2) {
+                // scaled terms of both pairs added first, then to the
+                // accumulator: one dependent add per step on acc[t]
+                const float2 sum = __fadd2_rn(V[0], V[1]);
+                V[0] = __fadd2_rn(V[0], D[0]);
+                V[1] = __fadd2_rn(V[1], D[1]);
+                acc[t] = __fadd2_rn(acc[t], sum);
+            } else if constexpr (PD_STEP_ORDER == 0 || PD_STEP_ORDER == 2) {
 #pragma unroll
                 for (int p = 0; p < NP; ++p) {
                     if constexpr (SCALED)
