@@ -143,6 +143,10 @@ int pd_router_wait(pd_router *r, uint64_t ticket, int timeout_ms, double *out_te
     if (rc != PD_ETIMEOUT || pd_poll(c, ct) != 0) {
         if (it != r->tickets.end()) r->settle_locked(it->second);
     }
+    // a result handed out (or a final failure) ends the ticket on the router
+    // too; a wait that only timed out keeps it
+    if (it != r->tickets.end() && (rc == PD_OK || (rc != PD_ETIMEOUT && out_terms)))
+        r->tickets.erase(it);
     if (rc != PD_OK) router_fail(rc, std::string("pd_router_wait: ") + pd_last_error(c));
     return rc;
 }

@@ -44,8 +44,11 @@ def test_two_replicas_on_one_device_match_solo_solves():
     router = Router([0, 0])
     try:
         tickets = [router.submit(r) for r in reqs]
-        outs = [router.wait(t, timeout_s=120) for t in tickets]
         replicas = {router.replica(t) for t in tickets}
+        outs = [router.wait(t, timeout_s=120) for t in tickets]
+        # a ticket whose result was taken is gone from the router
+        with pytest.raises(Exception):
+            router.replica(tickets[0])
     finally:
         router.close()
     assert replicas == {0, 1}
