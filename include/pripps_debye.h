@@ -56,9 +56,10 @@ extern "C" {
 
 /* ---- request flags ----
  * PD_FLAG_TEST_EXPIRED_WAIT is a test hook for the failure path of the FP32
- * pair kernel: the first tile taken by its first CTA waits for a bulk copy
- * of atoms that is never issued, with a short poll limit, so that the bounded
- * wait expires with no copy in flight. That CTA then stops, writes NaN to the
+ * pair kernel: the CTA that takes the first tile of a launch (when that tile
+ * belongs to a flagged request) waits for a bulk copy of atoms that is never
+ * issued, with a short poll limit, so that the bounded wait expires with no
+ * copy in flight. That CTA then stops, writes NaN to the
  * slots of every tile it still takes and sets the request's device status;
  * blocking calls (pd_solve, pd_plan_execute_host, pd_wait, pd_stream_finish)
  * return PD_ETIMEOUT, calls that leave the result on the device show NaN

@@ -61,7 +61,7 @@ constexpr int64_t PD_SLOT_MASK = (int64_t{1} << PD_SLOT_MAP_SHIFT) - 1;
 constexpr int32_t PD_DEV_WAIT_EXPIRED = 1;  // a bounded wait for a bulk copy gave up
 
 // PdReqDev::flags
-constexpr int32_t PD_REQF_TEST_EXPIRE = 1;  // test hook: CTA 0 skips its first copy
+constexpr int32_t PD_REQF_TEST_EXPIRE = 1;  // test hook: the launch's first tile skips its copy
 
 // Per-request descriptor read by the pair kernels.
 struct PdReqDev {

@@ -675,7 +675,7 @@ __global__ void __launch_bounds__(PD_THREADS, fp32_min_blocks(K, MODE, NP))
     // the slots of every tile it still takes and flags each tile's request
     // in its status word. This state lives in shared memory, not registers,
     // so that it adds nothing to the register pressure of the steps.
-    __shared__ int s_dead, s_first, s_polls, s_skip;
+    __shared__ int s_dead, s_polls, s_skip;
     __shared__ uint32_t s_inflight, s_par;  // thread 0: copies in flight, their parities
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
@@ -685,7 +685,6 @@ __global__ void __launch_bounds__(PD_THREADS, fp32_min_blocks(K, MODE, NP))
         mbar_init(&s_bar[1], 1);
         mbar_init_fence();
         s_dead = 0;
-        s_first = 1;
     }
     __syncthreads();
     uint32_t phase = 0;  // bit b: parity of buffer b's next completion
@@ -715,12 +714,11 @@ __global__ void __launch_bounds__(PD_THREADS, fp32_min_blocks(K, MODE, NP))
         }
         const int rchunk = (nres + 15) >> 4;
         if (threadIdx.x == 0) {
-            // test hook: the first tile of CTA 0 waits for a copy that is
-            // never issued, briefly, so that its wait expires with no copy in
-            // flight
-            s_skip = (rq.flags & PD_REQF_TEST_EXPIRE) != 0 && blockIdx.x == 0 && s_first;
+            // test hook: the CTA that takes the launch's first tile waits for
+            // a copy that is never issued, briefly, so that its wait expires
+            // with no copy in flight
+            s_skip = (rq.flags & PD_REQF_TEST_EXPIRE) != 0 && jid == 0;
             s_polls = s_skip ? PD_TEST_WAIT_POLLS : PD_WAIT_POLLS;
-            s_first = 0;
             s_inflight = 0;
             s_par = 0;
         }

@@ -3,7 +3,7 @@ faulting or hanging the GPU.
 
 The FP32 pair kernel stages atoms into shared memory with bulk copies and
 waits for each on an mbarrier, giving up after a poll limit. The request flag
-PD_FLAG_TEST_EXPIRED_WAIT makes the first tile of the kernel's first CTA wait
+PD_FLAG_TEST_EXPIRED_WAIT makes the CTA that takes a launch's first tile wait
 for a copy that is never issued, with a short limit, so the wait expires with
 nothing in flight. The reference turns a lost device into Error::Internal
 rather than a silent result (src/gpu.rs:577-621); here every blocking entry
