@@ -1,7 +1,7 @@
 // Device kernels of the Debye backend (sm_100a).
 //
 // K1 (pd_pairs_fp32): for each tile (i-block × j-range × q-block) every thread
-// owns one i atom and walks the j atoms of the range two at a time. For a pair
+// owns one i atom and walks the j atoms of the range NP at a time. For a pair
 // at distance r it needs sin(q_k r) for the K consecutive grid points
 // q_k = q_s + k·Δq of the block. With x = Δq·r reduced as x = mπ + x'
 // (|x'| <= π/2) the sequence is s_k = σ^k·u_k, σ = (-1)^m, where
@@ -12,9 +12,11 @@
 // recurrence; errors grow linearly in k). It is reseeded every K steps from
 // sin θ and cos θ evaluated in FP32 with a double-float phase and our own
 // fitted polynomials (see sincos_poly). One step plus the accumulation
-// acc_k += σ^k u_k / r is FFMA + FADD + FFMA, all on the FP32 pipes. acc_k
-// sums sin(q_k r)/r over the thread's pairs; dividing by q_k in FP64
-// afterwards gives Σ sinc(q_k r).
+// acc_k += σ^k u_k / r is FFMA + FADD + FADD, all on the FP32 pipes (the
+// weight 1/r scales the pair's initial u and d, and the pairs' terms are
+// summed before they reach acc_k; with the general step, σ alternating, the
+// accumulation is an FFMA with ±1/r). acc_k sums sin(q_k r)/r over the
+// thread's pairs; dividing by q_k in FP64 afterwards gives Σ sinc(q_k r).
 // Per-sub-chunk sums stay in FP32 registers; they are warp-reduced into FP64
 // partial sums in shared memory, merged per atom class at the end of the
 // tile into FP64 slots, and every later sum is FP64.
