@@ -40,11 +40,15 @@ UNIT = "pair·q/s"
 # 2) and the v-step (FADD, 1) of the recurrence, and the accumulation — an add
 # of terms whose weight 1/r the recurrence state already carries (FADD, 1) when
 # Δq·(largest pair distance) <= π/4, else an FFMA with the weight (2).
-# Weighted mode: the same step plus two weighted accumulations (FFMA + FFMA).
-FLOPS_PER_PAIRQ = {"class": 4, "class_general_step": 5, "weighted": 7}
-# FP32 pipe slots (lane operations) of one pair·q: three in every mode but
-# the weighted one (four).
-SLOTS_PER_PAIRQ = {"class": 3, "class_general_step": 3, "weighted": 4}
+# Weighted mode (a weight per atom): the same step and a second accumulator
+# of the terms times w_j (FFMA, 2); with the general step both accumulations
+# are FFMAs with the weight.
+FLOPS_PER_PAIRQ = {"class": 4, "class_general_step": 5, "weighted": 6,
+                   "weighted_general_step": 7}
+# FP32 pipe slots (lane operations) of one pair·q: three with one
+# accumulator, four with two.
+SLOTS_PER_PAIRQ = {"class": 3, "class_general_step": 3, "weighted": 4,
+                   "weighted_general_step": 4}
 PROFILES = ("atoms", "excluded", "hydration", "atom_excluded", "atom_hydration",
             "excluded_hydration")
 
@@ -402,18 +406,7 @@ def run_ours(args, ws, rank, local):
         secondary = run_secondary(ctx, args, local)
 
     if rank == 0:
-        mode = "class"
-        if req.hyd_weights is not None:
-            keys = set(zip(req.species.tolist(), req.hyd_weights.tolist()))
-            mode = "weighted" if len(keys) > 48 else "class"
-        if mode == "class":
-            # the kernel's test: Δq·2·(largest distance from the centroid) > 0.78
-            xyz = req.xyz.reshape(-1, req.n_atoms, 3)
-            radius = max(float(np.sqrt(((f - f.mean(axis=0)) ** 2).sum(axis=1)).max())
-                         for f in xyz)
-            dq = (req.qmax - req.qmin) / max(req.nq - 1, 1)
-            if dq * 2.0 * radius > 0.78:
-                mode = "class_general_step"
+        mode = kernel_mode(req)
         flops = FLOPS_PER_PAIRQ[mode]
         slots = SLOTS_PER_PAIRQ[mode]
         launch_ms = pair_ms.value / max(n_pair.value, 1)
@@ -460,10 +453,11 @@ def run_ours(args, ws, rank, local):
                              "frac": slots * kernel_pair_q / (launch_ms * 1e-3) / 1e12 /
                                      (peak / 2.0),
                              "note": "the kernel is bound by FP32 pipe slots: each pair·q "
-                                     "takes three FP32 lane operations (FFMA, FADD, FADD); "
-                                     "an FADD fills a slot for 1 FLOP, so the FLOP "
-                                     "fraction of this recurrence tops out at 4/6 of the "
-                                     "FFMA peak and the slot fraction at 1"},
+                                     f"takes {slots} FP32 lane operations ({mode} mode) "
+                                     f"for {flops} FLOP; an FADD fills a slot for 1 FLOP, "
+                                     "so the FLOP fraction tops out at "
+                                     f"{flops}/{2 * slots} of the FFMA peak and the slot "
+                                     "fraction at 1"},
                          "kernel_pair_q_per_launch": kernel_pair_q,
                          "kernel_ms_per_launch": launch_ms,
                          "peak_source": "measured FFMA probe (pd_measure_fp32_peak), best of "
@@ -498,6 +492,23 @@ def run_ours(args, ws, rank, local):
     if ws > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
+
+
+def kernel_mode(req):
+    """The pair kernel's mode for a request, as the planner picks it: class
+    mode while at most 48 (species, hydration weight) keys exist, else
+    weighted; "_general_step" where Δq·2·(largest distance from the
+    centroid) > 0.78."""
+    mode = "class"
+    if req.hyd_weights is not None:
+        keys = set(zip(req.species.tolist(), req.hyd_weights.tolist()))
+        mode = "weighted" if len(keys) > 48 else "class"
+    xyz = req.xyz.reshape(-1, req.n_atoms, 3)
+    radius = max(float(np.sqrt(((f - f.mean(axis=0)) ** 2).sum(axis=1)).max()) for f in xyz)
+    dq = (req.qmax - req.qmin) / max(req.nq - 1, 1)
+    if dq * 2.0 * radius > 0.78:
+        mode += "_general_step"
+    return mode
 
 
 def timed_workload(ctx, w, local, min_seconds=2.0):
@@ -582,9 +593,11 @@ def run_secondary(ctx, args, local):
     record, and a 400-request serving burst."""
     from pripps_b200 import workloads
     out = {}
-    for name in ("sphere_solvent_10k", "trajectory_5k_256"):
+    for name in ("sphere_solvent_10k", "trajectory_5k_256", "ellipsoid_sasa_20k"):
         if name != args.workload:
-            out[name] = timed_workload(ctx, workloads.WORKLOADS[name](args.precision), local)
+            w = workloads.WORKLOADS[name](args.precision)
+            out[name] = timed_workload(ctx, w, local)
+            out[name]["kernel_mode"] = kernel_mode(w.request)
     out["serving_burst_400"] = serving_burst(ctx, local, 400, args.precision)
     return out
 

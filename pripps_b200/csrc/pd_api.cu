@@ -309,7 +309,7 @@ Tuning tuning_for(pd_ctx *ctx, int64_t n, int64_t nq, int precision, int64_t n_f
             return it->second.t;
         }
     }
-    return pd::default_tuning(n, nq, precision, n_frames);
+    return pd::fit_tuning(precision, mode, pd::default_tuning(n, nq, precision, n_frames));
 }
 
 Tuning tuning_for_request(pd_ctx *ctx, const pd_request *req, const uint32_t *species,
@@ -1708,7 +1708,7 @@ std::vector<Tuning> tune_candidates(const pd_request *req, int mode) {
     if (precision == PD_FP64)
         shapes = {{16, 1}, {32, 1}};
     else if (mode == PD_MODE_WEIGHTED)
-        shapes = {{32, 2}, {64, 2}};
+        shapes = {{32, 2}, {64, 2}, {64, 4}};
     else if (nq <= 32)
         shapes = {{32, 4}};
     else
@@ -1720,7 +1720,10 @@ std::vector<Tuning> tune_candidates(const pd_request *req, int mode) {
         if (std::find(tjs.begin(), tjs.end(), tj) == tjs.end()) tjs.push_back(tj);
     }
     std::vector<Tuning> out;
-    const Tuning def = pd::default_tuning(n, nq, precision, static_cast<int64_t>(req->n_frames));
+    // every candidate as the planner would run it, so the table records the
+    // shape that was timed
+    const Tuning def = pd::fit_tuning(
+        precision, mode, pd::default_tuning(n, nq, precision, static_cast<int64_t>(req->n_frames)));
     out.push_back(def);
     for (auto sh : shapes)
         for (int tj : tjs) {

@@ -17,6 +17,9 @@
 // summed before they reach acc_k; with the general step, σ alternating, the
 // accumulation is an FFMA with ±1/r). acc_k sums sin(q_k r)/r over the
 // thread's pairs; dividing by q_k in FP64 afterwards gives Σ sinc(q_k r).
+// With a hydration weight per atom (weighted mode) a second accumulator sums
+// the terms times w_j (one more FFMA). Both modes run the even and odd grid
+// points of a pair as the two halves of packed FP32x2 instructions.
 // Per-sub-chunk sums stay in FP32 registers; they are warp-reduced into FP64
 // partial sums in shared memory, merged per atom class at the end of the
 // tile into FP64 slots, and every later sum is FP64.
@@ -394,7 +397,7 @@ struct SeedGroup {
                                          float qs_lo, float dq_hi, float dq_lo) {
         vsum = 0.0f;
         vwsum = 0.0f;
-        if constexpr (PD_SEED_X2 && MODE == PD_MODE_CLASS && NP % 2 == 0) {
+        if constexpr (PD_SEED_X2 && NP % 2 == 0) {
 #pragma unroll
             for (int p = 0; p < NP; p += 2) {
                 const int ja = j + p, jb = j + p + 1;
@@ -404,7 +407,17 @@ struct SeedGroup {
                 const bool va = ivalid && ina && (ja > i), vb = ivalid && inb && (jb > i);
                 pair_seed_x2<GENERAL_STEP>(pi, pja, pjb, va, vb, qs_hi, qs_lo, dq_hi, dq_lo,
                                            S[p], S[p + 1]);
-                if (RESID) vsum += (va ? 1.0f : 0.0f) + (vb ? 1.0f : 0.0f);
+                if (MODE == PD_MODE_WEIGHTED) {
+                    wj[p] = pja.w;
+                    wj[p + 1] = pjb.w;
+                }
+                if (RESID) {
+                    vsum += (va ? 1.0f : 0.0f) + (vb ? 1.0f : 0.0f);
+                    if (MODE == PD_MODE_WEIGHTED) {
+                        vwsum += va ? pja.w : 0.0f;
+                        vwsum += vb ? pjb.w : 0.0f;
+                    }
+                }
             }
             return;
         }
@@ -598,6 +611,85 @@ __device__ __forceinline__ void pairs_range_x2(const float4 *__restrict__ at, in
     }
 }
 
+// Weighted mode on packed FP32x2 instructions: the same chains as
+// pairs_range_x2 with two accumulators per grid point, Σ w d/r-terms (acc0)
+// and Σ w_j·terms (acc1). Without the general step the weight 1/r rides in
+// v and d (SCALED), acc0 takes the pairs' terms summed among themselves and
+// acc1 one FFMA2 per pair with w_j: four FP32 lane slots per pair·q (d-step,
+// v-step, the two accumulations), on half the issue slots of the scalar
+// form.
+#ifndef PD_WEIGHTED_X2
+#define PD_WEIGHTED_X2 1
+#endif
+template <int K, int NP, bool RESID, bool GENERAL_STEP>
+__device__ __forceinline__ void pairs_range_x2w(const float4 *__restrict__ at, int jbase,
+                                                float4 pi, int i, bool ivalid, int j0, int j1,
+                                                float qs_hi, float qs_lo, float dq_hi,
+                                                float dq_lo, const float2 *__restrict__ s_qres2,
+                                                float2 (&acc0)[K / 2], float2 (&acc1)[K / 2],
+                                                int nchunk, int rchunk = K / 16) {
+    static_assert(K % 16 == 0, "K must be a multiple of 16");
+    if (j0 >= j1) return;
+    constexpr bool SCALED = PD_SCALED_V && !GENERAL_STEP;
+    SeedGroup<PD_MODE_WEIGHTED, NP, RESID, GENERAL_STEP> cur;
+    cur.make(at, jbase, pi, i, ivalid, j0, j1, qs_hi, qs_lo, dq_hi, dq_lo);
+    for (int j = j0; j < j1; j += NP) {
+        float2 V[NP], D[NP], NA[NP], WJ[NP], WE[NP], WO[NP], WJE[NP], WJO[NP];
+#pragma unroll
+        for (int p = 0; p < NP; ++p) {
+            const float w = cur.S[p].we;
+            if (SCALED) {
+                V[p] = make_float2(w * cur.S[p].ve, w * cur.S[p].vo);
+                D[p] = make_float2(w * cur.S[p].de, w * cur.S[p].dd);
+                WJ[p] = make_float2(cur.wj[p], cur.wj[p]);
+            } else {
+                V[p] = make_float2(cur.S[p].ve, cur.S[p].vo);
+                D[p] = make_float2(cur.S[p].de, cur.S[p].dd);
+                const float wo = cur.S[p].wo;
+                WE[p] = make_float2(w, w);
+                WO[p] = make_float2(wo, wo);
+                WJE[p] = make_float2(w * cur.wj[p], w * cur.wj[p]);
+                WJO[p] = make_float2(wo * cur.wj[p], wo * cur.wj[p]);
+            }
+            NA[p] = make_float2(cur.S[p].na, cur.S[p].na);
+        }
+        const float2 mvs = make_float2(-cur.vsum, -cur.vsum);
+        const float2 mvws = make_float2(-cur.vwsum, -cur.vwsum);
+        cur.make(at, jbase, pi, i, ivalid, j + NP, j1, qs_hi, qs_lo, dq_hi, dq_lo);
+        int qoff = 0;  // opaque zero: keeps the K/2 q loads in the loop
+        if (RESID) asm volatile("mov.b32 %0, %0;" : "+r"(qoff));
+#pragma unroll
+        for (int t = 0; t < K / 2; ++t) {
+            if ((t % PD_CHUNK_T) == 0 && t / PD_CHUNK_T >= nchunk) break;
+            if (RESID && (t / 8) < rchunk) {
+                const float2 q2 = s_qres2[t + qoff];
+                acc0[t] = __ffma2_rn(mvs, q2, acc0[t]);
+                acc1[t] = __ffma2_rn(mvws, q2, acc1[t]);
+            }
+#pragma unroll
+            for (int p = 0; p < NP; ++p) D[p] = __ffma2_rn(NA[p], V[p], D[p]);
+            if constexpr (SCALED) {
+                float2 sum = V[0];
+#pragma unroll
+                for (int p = 1; p < NP; ++p) sum = __fadd2_rn(sum, V[p]);
+                float2 a1 = acc1[t];
+#pragma unroll
+                for (int p = 0; p < NP; ++p) a1 = __ffma2_rn(WJ[p], V[p], a1);
+                acc1[t] = a1;
+                acc0[t] = __fadd2_rn(acc0[t], sum);
+            } else {
+#pragma unroll
+                for (int p = 0; p < NP; ++p) {
+                    acc0[t] = __ffma2_rn((t & 1) ? WO[p] : WE[p], V[p], acc0[t]);
+                    acc1[t] = __ffma2_rn((t & 1) ? WJO[p] : WJE[p], V[p], acc1[t]);
+                }
+            }
+#pragma unroll
+            for (int p = 0; p < NP; ++p) V[p] = __fadd2_rn(V[p], D[p]);
+        }
+    }
+}
+
 // Pairs a thread adds in FP32 before the warp's partial sums go into its
 // FP64 slot. A j range of a tile is walked in sub-chunks of this length with
 // fresh FP32 accumulators: FP32 running sums over thousands of terms lose
@@ -629,6 +721,29 @@ constexpr int fp32_min_blocks(int K, int MODE, int NP) {
 // issued.
 constexpr int PD_WAIT_POLLS = 1 << 22;
 constexpr int PD_TEST_WAIT_POLLS = 1 << 10;
+
+// Weighted-mode flush of one accumulator array: the warp sums of acc and of
+// w_i·acc, reduce-scattered (lane l ends with grid points
+// [l·K/32, (l+1)·K/32)) and added to part[k] and part[K + k].
+template <int K>
+__device__ __forceinline__ void flush_weighted_rs(float2 (&acc)[K / 2], float wi,
+                                                  double *__restrict__ part, int lane,
+                                                  bool first) {
+    const float2 wi2 = make_float2(wi, wi);
+    float2 tw[K / 2];
+#pragma unroll
+    for (int t = 0; t < K / 2; ++t) tw[t] = __fmul2_rn(wi2, acc[t]);
+    warp_reduce_scatter<K / 2>(acc, lane);
+    warp_reduce_scatter<K / 2>(tw, lane);
+#pragma unroll
+    for (int m = 0; m < K / 32; ++m) {
+        const int k = lane * (K / 32) + m;
+        const float s = (m & 1) ? acc[m >> 1].y : acc[m >> 1].x;
+        const float sw = (m & 1) ? tw[m >> 1].y : tw[m >> 1].x;
+        part[k] = (first ? 0.0 : part[k]) + static_cast<double>(s);
+        part[K + k] = (first ? 0.0 : part[K + k]) + static_cast<double>(sw);
+    }
+}
 
 // End of a tile: the warps' FP64 partial sums (part[w·nvk + e], e < nvk) of
 // one class are added in warp order and written to that class's slot; a CTA
@@ -663,6 +778,8 @@ __global__ void __launch_bounds__(PD_THREADS, fp32_min_blocks(K, MODE, NP))
     constexpr int NACC = (MODE == PD_MODE_WEIGHTED) ? 2 : 1;
     constexpr int NV = (MODE == PD_MODE_WEIGHTED) ? 4 : 1;  // FP64 values per q in a slot
     constexpr bool PACKED = (MODE == PD_MODE_CLASS);
+    constexpr bool PACKED_W =
+        (MODE == PD_MODE_WEIGHTED) && PD_WEIGHTED_X2 && (K / 2) % 32 == 0 && NP % 2 == 0;
     __shared__ int s_job;
     __shared__ __align__(16) float s_qres[K];
     // per-warp FP64 partial sums of the current tile, [warp][NV][K]
@@ -823,6 +940,40 @@ __global__ void __launch_bounds__(PD_THREADS, fp32_min_blocks(K, MODE, NP))
                                     (first ? 0.0 : part[2 * t + 1]) + static_cast<double>(v1);
                         }
                         }
+                    } else if constexpr (PACKED_W) {
+                        const float2 *q2 = reinterpret_cast<const float2 *>(s_qres);
+                        const int nchunk =
+                            (min(K, rq.nq - kq0) + 2 * PD_CHUNK_T - 1) / (2 * PD_CHUNK_T);
+                        float2 acc0[K / 2], acc1[K / 2];
+#pragma unroll
+                        for (int t = 0; t < K / 2; ++t) {
+                            acc0[t] = make_float2(0.0f, 0.0f);
+                            acc1[t] = make_float2(0.0f, 0.0f);
+                        }
+                        if (resid) {
+                            if (general_step)
+                                pairs_range_x2w<K, NP, true, true>(
+                                    chunk, jss, pi, i, ivalid, js, je, qs_hi, qs_lo, dq_hi, dq_lo,
+                                    q2, acc0, acc1, K / (2 * PD_CHUNK_T), rchunk);
+                            else
+                                pairs_range_x2w<K, NP, true, false>(
+                                    chunk, jss, pi, i, ivalid, js, je, qs_hi, qs_lo, dq_hi, dq_lo,
+                                    q2, acc0, acc1, K / (2 * PD_CHUNK_T), rchunk);
+                        } else {
+                            if (general_step)
+                                pairs_range_x2w<K, NP, false, true>(chunk, jss, pi, i, ivalid, js,
+                                                                    je, qs_hi, qs_lo, dq_hi, dq_lo,
+                                                                    q2, acc0, acc1, nchunk);
+                            else
+                                pairs_range_x2w<K, NP, false, false>(
+                                    chunk, jss, pi, i, ivalid, js, je, qs_hi, qs_lo, dq_hi, dq_lo,
+                                    q2, acc0, acc1, nchunk);
+                        }
+                        // the four warp sums of each grid point: Σ acc0,
+                        // Σ w_i·acc0, Σ acc1, Σ w_i·acc1
+                        const float wi = ivalid ? pi.w : 0.0f;
+                        flush_weighted_rs<K>(acc0, wi, part, lane, first);
+                        flush_weighted_rs<K>(acc1, wi, part + 2 * K, lane, first);
                     } else {
                         const float wi = ivalid ? pi.w : 0.0f;
                         float acc[NACC][K];
@@ -1784,7 +1935,7 @@ static int occupancy_fp64() {
 // accumulators per q) only up to K = 64 to stay within 255 registers.
 bool valid_shape(int precision, int mode, int K, int NP) {
     if (precision == 1) return (K == 16 || K == 32) && NP == 1;
-    if (mode == PD_MODE_WEIGHTED) return (K == 32 && NP == 2) || (K == 64 && NP == 2);
+    if (mode == PD_MODE_WEIGHTED) return (K == 32 && NP == 2) || (K == 64 && (NP == 2 || NP == 4));
     return (K == 32 && NP == 4) || (K == 64 && NP >= 1 && NP != 3) || (K == 96 && NP == 2) ||
            (K == 128 && NP >= 1 && NP != 3) || ((K == 160 || K == 192) && NP == 1);
 }
@@ -1809,7 +1960,7 @@ cudaError_t launch_pairs(int precision, int K_, int NP_, int mode, const PdJob *
     }
     PD_F32(32, 0, 4) PD_F32(64, 0, 1) PD_F32(64, 0, 2) PD_F32(64, 0, 4) PD_F32(96, 0, 2)
     PD_F32(128, 0, 1) PD_F32(128, 0, 2) PD_F32(128, 0, 4) PD_F32(160, 0, 1) PD_F32(192, 0, 1)
-    PD_F32(32, 1, 2) PD_F32(64, 1, 2)
+    PD_F32(32, 1, 2) PD_F32(64, 1, 2) PD_F32(64, 1, 4)
     return cudaErrorInvalidValue;
 }
 
@@ -1825,14 +1976,15 @@ int pairs_blocks_per_sm(int precision, int K_, int NP_, int mode) {
     }
     PD_O32(32, 0, 4) PD_O32(64, 0, 1) PD_O32(64, 0, 2) PD_O32(64, 0, 4) PD_O32(96, 0, 2)
     PD_O32(128, 0, 1) PD_O32(128, 0, 2) PD_O32(128, 0, 4) PD_O32(160, 0, 1) PD_O32(192, 0, 1)
-    PD_O32(32, 1, 2) PD_O32(64, 1, 2)
+    PD_O32(32, 1, 2) PD_O32(64, 1, 2) PD_O32(64, 1, 4)
     return 0;
 }
 
 cudaError_t prepare_pair_kernels() {
     const int shapes[][3] = {{32, 0, 4},  {64, 0, 1},  {64, 0, 2},  {64, 0, 4},
                              {96, 0, 2},  {128, 0, 1}, {128, 0, 2}, {128, 0, 4},
-                             {160, 0, 1}, {192, 0, 1}, {32, 1, 2},  {64, 1, 2}};
+                             {160, 0, 1}, {192, 0, 1}, {32, 1, 2},  {64, 1, 2},
+                             {64, 1, 4}};
     for (const auto &sh : shapes)
         if (pairs_blocks_per_sm(0, sh[0], sh[2], sh[1]) <= 0) return cudaErrorInvalidValue;
     return cudaSuccess;

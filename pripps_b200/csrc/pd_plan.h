@@ -73,6 +73,9 @@ int validate_request(const pd_request *req, bool device_pointers, std::string &m
 
 // Default shape when no tuned entry exists.
 Tuning default_tuning(int64_t n_atoms, int64_t nq, int precision, int64_t n_frames = 1);
+// The instantiated kernel shape a requested one runs as in a mode (the q
+// block and pairs per thread adjusted where that shape has no kernel).
+Tuning fit_tuning(int precision, int mode, Tuning t);
 
 // A rank's share of a plan for a tile-sharded solve: every world-th tile of
 // the cost-ordered job list, with only the slots those tiles write (numbered

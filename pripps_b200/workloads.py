@@ -1,10 +1,13 @@
-"""The five Debye workloads, built from seeded synthetic globules.
+"""The Debye workloads, built from seeded synthetic globules.
 
   sphere_vacuum_1k     1,000 atoms, sphere R = 16 Å, vacuum, q ∈ [0, 0.5], nq = 500
   sphere_solvent_10k   10,000 atoms, sphere R = 35 Å, FoXS Fraser excluded volume
                        + Bernoulli(0.35) surface hydration, q ∈ [0, 0.5], nq = 500
   ellipsoid_solvent_100k  100,000 atoms, prolate ellipsoid 80×40×40 Å, solvent as
                        above, q ∈ [0, 1.0], nq = 1,000
+  ellipsoid_solvent_20k / ellipsoid_sasa_20k  20,000 atoms at the 100k density,
+                       nq = 512; the second with a continuous hydration weight
+                       per atom (SASA-like: weighted mode)
   trajectory_5k_256    256 frames of a 5,000-atom sphere (R = 25 Å), σ = 0.5 Å,
                        Dirichlet(1) frame weights, vacuum, q ∈ [0, 0.5], nq = 300
   stream               Poisson requests, N log-uniform 500–50,000 (sphere at the
@@ -124,6 +127,19 @@ def ellipsoid_solvent_20k(precision="fp32") -> Workload:
                     globule_request(g, 0.0, 1.0, 512, True, precision), g)
 
 
+def ellipsoid_sasa_20k(precision="fp32") -> Workload:
+    """The 20,000-atom ellipsoid with a hydration weight per atom, as pripps'
+    SASA hydration gives (area × shell thickness / water volume, a continuous
+    value): each exposed atom's full-shell weight times a seeded exposed
+    fraction in [0.05, 1). With thousands of distinct weights the kernels run
+    in weighted mode (two accumulators per q)."""
+    w = ellipsoid_solvent_20k(precision)
+    req = w.request
+    rng = np.random.default_rng(20)
+    req.hyd_weights = req.hyd_weights * rng.uniform(0.05, 1.0, req.n_atoms)
+    return Workload("ellipsoid_sasa_20k", req, w.globule)
+
+
 def trajectory_5k_256(precision="fp32", n_frames: int = 256) -> Workload:
     g = _globule(5000, (25.0, 25.0, 25.0), 3)
     frames, w = synth.trajectory(g.pos, n_frames, 0.5, 3)
@@ -226,5 +242,6 @@ WORKLOADS = {
     "sphere_solvent_10k": sphere_solvent_10k,
     "ellipsoid_solvent_100k": ellipsoid_solvent_100k,
     "ellipsoid_solvent_20k": ellipsoid_solvent_20k,
+    "ellipsoid_sasa_20k": ellipsoid_sasa_20k,
     "trajectory_5k_256": trajectory_5k_256,
 }

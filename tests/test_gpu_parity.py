@@ -130,6 +130,45 @@ def test_fp32_every_kernel_shape(gpu_ctx, shape):
         ctx.close()
 
 
+@pytest.mark.parametrize("shape", [(32, 2), (64, 2), (64, 4)])
+@pytest.mark.parametrize("grid", ["small_q_first_block", "general_step"])
+def test_fp32_weighted_every_kernel_shape(tmp_path, shape, grid):
+    """Weighted mode (a hydration weight per atom, as SASA areas give: more
+    distinct (species, weight) keys than classes) in each instantiated shape
+    against the oracle: once on a grid whose first block sits in the small-q
+    residual form, once with a step Δq·2R > π/4 (the general step)."""
+    K, NP = shape
+    if grid == "small_q_first_block":
+        w = workloads.small_globule(2500, 23, nq=300, qmax=0.7, precision="fp32")
+        qi = np.array([0, 1, 2, 3, K - 1, K, K + 1, 150, 299])
+    else:
+        w = workloads.small_globule(2500, 29, nq=60, qmax=3.0, precision="fp32")
+        qi = np.arange(0, 60, 7)
+    rng = np.random.default_rng(K + NP)
+    req = w.request
+    req.hyd_weights = req.hyd_weights * rng.uniform(0.05, 1.0, req.n_atoms)
+    assert len(np.unique(req.hyd_weights)) > 100
+    nq_log2 = int(np.log2(req.nq))
+    p = tmp_path / "tune.txt"
+    p.write_text(f"fp32 weighted single 11 {nq_log2} {K} 512 {NP} 1.0\n")
+    ctx = _lib.Context(0)
+    try:
+        _lib.check(_lib.lib().pd_tuning_load(ctx.handle, str(p).encode()), ctx.handle)
+        plan = C.c_void_p()
+        r = req.c_struct()
+        _lib.check(_lib.lib().pd_plan_create(ctx.handle, C.byref(r), C.byref(plan)), ctx.handle)
+        k, tj, np_ = C.c_uint32(), C.c_uint32(), C.c_uint32()
+        _lib.check(_lib.lib().pd_plan_info(plan, C.byref(k), C.byref(tj), C.byref(np_), None,
+                                           None, None), None)
+        _lib.lib().pd_plan_destroy(ctx.handle, plan)
+        assert (k.value, np_.value) == (K, NP)
+        t = solve(req, ctx)
+        ref = O.terms_for_request(req, q_index=qi, precise=True)
+        assert np.all(term_errors(t[:, qi], ref) < 1e-5)
+    finally:
+        ctx.close()
+
+
 def test_fp32_small_q_bias(gpu_ctx):
     """Many nearly equal terms: 30,000 atoms in a compact ball at q ≤ 0.01,
     where every sin(q r)/r ≈ q. Sequential FP32 sums of such terms round with

@@ -91,6 +91,20 @@ def test_lookup_without_context_uses_the_shipped_table():
         assert not tab64 and shape64[2] == 1  # the FP64 kernel runs one pair per pass
 
 
+def test_weighted_default_is_a_weighted_kernel_shape():
+    """A weighted-mode request (a distinct hydration weight per atom) in a
+    bucket no table names gets a shape the weighted kernels have — the one
+    its plan runs — not the class-mode default."""
+    if os.environ.get("PRIPPS_DEBYE_TUNING"):
+        pytest.skip("a tuning file other than the shipped one is in use")
+    w = workloads.small_globule(300, 7, nq=300)  # 2^8 <= 300 < 2^9: no weighted entry
+    req = w.request
+    req.hyd_weights = np.linspace(0.1, 2.0, req.n_atoms)
+    shape, from_table = lookup(req)
+    assert not from_table
+    assert (shape[0], shape[2]) in {(32, 2), (64, 2), (64, 4)}
+
+
 @pytest.mark.gpu
 def test_loaded_table_drives_solves_and_plans(tmp_path):
     """A table entry for the request's bucket is what a plan gets, and the
