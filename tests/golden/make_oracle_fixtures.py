@@ -1,7 +1,8 @@
-"""Oracle fixtures of the two solvent workloads, for the -m gpu parity tests.
+"""Oracle fixtures of the solvent workloads, for the -m gpu parity tests.
 
     python tests/golden/make_oracle_fixtures.py sphere10k [--threads T]
     python tests/golden/make_oracle_fixtures.py ellipsoid100k [--threads T] [--q-index i,j,...]
+    python tests/golden/make_oracle_fixtures.py sasa20k [--threads T]
 
 Runs the FP64 CPU oracle in its compensated form (long double accumulators,
 the reference's loop structure of src/debye.rs:214-250 otherwise) on the
@@ -15,7 +16,13 @@ script:
   oracle_ellipsoid_solvent_100k.json
       100,000 atoms in an 80 × 40 × 40 Å prolate ellipsoid with the same
       solvent model, q ∈ [0, 1], nq = 1,000: all six profiles on a q subset
-      (about 37 CPU-minutes per point on one core).
+      (about 37 CPU-minutes per point on one core);
+  oracle_ellipsoid_sasa_20k.json
+      20,000 atoms at the same density with a continuous hydration weight per
+      atom (the kernels' weighted mode), q ∈ [0, 1], nq = 512: all six
+      profiles at q = 0, the small-q residual form, both sides of the first
+      64-point q-block seam, every minimum of the atoms profile (95 … 503;
+      located as for the 100k subset) and qmax.
 
 Each fixture carries a SHA-256 digest of the request's inputs (positions,
 species, form-factor tables, hydration weights), so a test can tell a
@@ -52,6 +59,7 @@ from oracle import oracle as O  # noqa: E402
 from pripps_b200 import workloads  # noqa: E402
 
 DEFAULT_100K = [0, 1, 2, 3, 72, 108, 127, 128, 186, 264, 500, 655, 812, 894, 965, 999]
+DEFAULT_SASA20K = [0, 1, 2, 3, 63, 64, 95, 164, 231, 300, 372, 436, 503, 511]
 
 
 def write(name: str, w, q_index, threads: int) -> Path:
@@ -82,7 +90,7 @@ def write(name: str, w, q_index, threads: int) -> Path:
 
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
-    ap.add_argument("which", choices=["sphere10k", "ellipsoid100k"])
+    ap.add_argument("which", choices=["sphere10k", "ellipsoid100k", "sasa20k"])
     ap.add_argument("--threads", type=int, default=0, help="oracle threads (0: all cores)")
     ap.add_argument("--q-index", default=None,
                     help="comma-separated grid indices (ellipsoid100k only)")
@@ -93,6 +101,9 @@ def main(argv=None):
     if args.which == "sphere10k":
         w = workloads.sphere_solvent_10k("fp64")
         p = write("oracle_sphere_solvent_10k.json", w, None, args.threads)
+    elif args.which == "sasa20k":
+        w = workloads.ellipsoid_sasa_20k("fp64")
+        p = write("oracle_ellipsoid_sasa_20k.json", w, np.array(DEFAULT_SASA20K), args.threads)
     else:
         qi = DEFAULT_100K if args.q_index is None else [int(s) for s in args.q_index.split(",")]
         w = workloads.ellipsoid_solvent_100k("fp64")

@@ -1,10 +1,14 @@
-"""The two solvent workloads against the CPU oracle itself, through the C ABI.
+"""The solvent workloads against the CPU oracle itself, through the C ABI.
 
 Fixtures (tests/golden/make_oracle_fixtures.py, compensated FP64 oracle):
   oracle_sphere_solvent_10k.json      10,000 atoms, nq = 500: the whole grid
   oracle_ellipsoid_solvent_100k.json  100,000 atoms, nq = 1,000: a q subset
                                       (q = 0, small q, the first and deepest
                                       minima, both sides of a q-block seam, qmax)
+  oracle_ellipsoid_sasa_20k.json      20,000 atoms with a hydration weight per
+                                      atom (weighted mode), nq = 512: q = 0,
+                                      small q, a q-block seam, every minimum of
+                                      the atoms profile, qmax
 
 Tolerances: PD_FP64 within 1e-10 and PD_FP32_FP64RED within 1e-5 on every
 profile; self profiles relative, cross profiles normalised by
@@ -24,6 +28,7 @@ FIXTURES = {
     "sphere_solvent_10k": ("oracle_sphere_solvent_10k.json", workloads.sphere_solvent_10k),
     "ellipsoid_solvent_100k": ("oracle_ellipsoid_solvent_100k.json",
                                workloads.ellipsoid_solvent_100k),
+    "ellipsoid_sasa_20k": ("oracle_ellipsoid_sasa_20k.json", workloads.ellipsoid_sasa_20k),
 }
 
 
