@@ -436,9 +436,12 @@ uint64_t pd_launch_count(pd_ctx *ctx);
  *    partial sums) needs more than PD_NOALLOC_SCRATCH_BYTES fails with
  *    PD_EBUDGET and a message naming both sizes, before any device work.
  *    pd_request_device_bytes(ctx, req, 0, &bytes) gives a request's need
- *    beforehand. As a guide, an FP32 solve of 100,000 atoms with solvent at
- *    nq = 1,000 fits (about 45 MB); 200,000 atoms at nq = 1,000 need about
- *    115 MB and are refused.
+ *    beforehand; the need depends on the atom classes as well as on N and
+ *    nq. As a guide, at nq = 1,000 an FP32 solve with solvent and one
+ *    hydration weight per element fits up to about 100,000 atoms (the
+ *    100,000-atom ellipsoid needs 59 MB, 110,000 atoms of it 71 MB) and
+ *    200,000 atoms are refused; with a hydration weight per atom (four
+ *    partial sums per grid point) the limit is about 60,000 atoms.
  *  - The array occupies PD_NOALLOC_SCRATCH_BYTES of memory on every GPU that
  *    loads the library's device code, until the process exits.
  *  - Every call shares the array, which keeps the previous call's contents;

@@ -123,15 +123,18 @@ def test_noalloc_refuses_requests_beyond_the_scratch():
 
 
 def test_noalloc_size_guide_holds():
-    """Host-only: the header's guide — an FP32 solve of 100,000 atoms with
-    solvent at nq = 1,000 fits the fixed scratch, 200,000 atoms at nq = 1,000
-    do not — checked on the layout the entry point computes."""
-    def need(n, nq):
+    """Host-only: the header's guide — at nq = 1,000 an FP32 solve of 100,000
+    atoms with solvent and one hydration weight per element fits the fixed
+    scratch and 200,000 atoms do not; with a weight per atom 60,000 atoms fit
+    and 70,000 do not — checked on the layout the entry point computes."""
+    def need(n, nq, per_atom_weights=False):
         rng = np.random.default_rng(n)
+        w = np.where(rng.random(n) < 0.3, 1.2, 0.0)
+        if per_atom_weights:
+            w = w * rng.uniform(0.05, 1.0, n)
         req = DebyeRequest(rng.uniform(-50, 50, (n, 3)), rng.integers(0, 4, n).astype(np.uint32),
                            rng.uniform(1, 8, (4, nq)), rng.uniform(0.5, 2, (4, nq)),
-                           np.where(rng.random(n) < 0.3, 1.2, 0.0), rng.uniform(5, 10, nq),
-                           0.0, 0.5, nq, None, "fp32")
+                           w, rng.uniform(5, 10, nq), 0.0, 0.5, nq, None, "fp32")
         r = req.c_struct()
         out = C.c_uint64()
         _lib.check(_lib.lib().pd_request_device_bytes(None, C.byref(r), 0, C.byref(out)), None,
@@ -139,6 +142,8 @@ def test_noalloc_size_guide_holds():
         return out.value
     assert need(100_000, 1000) <= _lib.PD_NOALLOC_SCRATCH_BYTES
     assert need(200_000, 1000) > _lib.PD_NOALLOC_SCRATCH_BYTES
+    assert need(60_000, 1000, True) <= _lib.PD_NOALLOC_SCRATCH_BYTES
+    assert need(70_000, 1000, True) > _lib.PD_NOALLOC_SCRATCH_BYTES
 
 
 def test_noalloc_rejects_missing_buffers():
