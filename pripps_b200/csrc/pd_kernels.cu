@@ -516,6 +516,28 @@ __device__ __forceinline__ void pairs_range(const float4 *__restrict__ at, int j
 #ifndef PD_SCALED_V
 #define PD_SCALED_V 1
 #endif
+// Where the seeds of a pass are computed. With K = 128 and four pairs per
+// thread each pass computes its own seeds before its steps: no next-pass
+// seeds are held through the steps, the kernel fits 168 registers and three
+// CTAs per SM instead of 255 and two, and the third warp per scheduler hides
+// the seeds' dependency chains (546.7 ms against 556.0 ms on the
+// 100,000-atom solve; with two CTAs per SM seeds at the top measured
+// 558.5 ms). Every other shape computes the next pass's seeds while the
+// current pass steps (it gains no CTA from the registers freed).
+#ifndef PD_SEED_TOP
+#define PD_SEED_TOP 1
+#endif
+template <int K, int NP>
+constexpr bool seeds_at_top() {
+    return PD_SEED_TOP && K == 128 && NP == 4;
+}
+#ifndef PD_SEED_TOP_W
+#define PD_SEED_TOP_W 0
+#endif
+template <int K, int NP>
+constexpr bool seeds_at_top_w() {
+    return PD_SEED_TOP_W && K == 64 && NP == 2;
+}
 // Instruction order within a step: 0 = d-steps, accumulations, v-steps;
 // 1 = d-steps, then per pair its accumulation and v-step; 2 (with
 // PD_SCALED_V, two or four pairs) = the pairs' scaled terms summed, then
@@ -540,8 +562,10 @@ __device__ __forceinline__ void pairs_range_x2(const float4 *__restrict__ at, in
     static_assert(K % 16 == 0, "K must be a multiple of 16");
     if (j0 >= j1) return;
     SeedGroup<PD_MODE_CLASS, NP, RESID, GENERAL_STEP> cur;
-    cur.make(at, jbase, pi, i, ivalid, j0, j1, qs_hi, qs_lo, dq_hi, dq_lo);
+    constexpr bool TOP = seeds_at_top<K, NP>();
+    if (!TOP) cur.make(at, jbase, pi, i, ivalid, j0, j1, qs_hi, qs_lo, dq_hi, dq_lo);
     for (int j = j0; j < j1; j += NP) {
+        if (TOP) cur.make(at, jbase, pi, i, ivalid, j, j1, qs_hi, qs_lo, dq_hi, dq_lo);
         // SCALED: without the general step every term of a pair has the
         // weight w = 1/r, which the linear recurrence can carry in v and d
         // themselves; the accumulation is then a plain add.
@@ -564,7 +588,7 @@ __device__ __forceinline__ void pairs_range_x2(const float4 *__restrict__ at, in
         const float2 mvs = make_float2(-cur.vsum, -cur.vsum);
         // the next pass's seeds (unused after the last pass), computed in
         // place while the steps below run on this pass's copies
-        cur.make(at, jbase, pi, i, ivalid, j + NP, j1, qs_hi, qs_lo, dq_hi, dq_lo);
+        if (!TOP) cur.make(at, jbase, pi, i, ivalid, j + NP, j1, qs_hi, qs_lo, dq_hi, dq_lo);
         int qoff = 0;  // opaque zero: keeps the K/2 q loads in the loop
         if (RESID) asm volatile("mov.b32 %0, %0;" : "+r"(qoff));
 #pragma unroll
@@ -632,8 +656,10 @@ __device__ __forceinline__ void pairs_range_x2w(const float4 *__restrict__ at, i
     if (j0 >= j1) return;
     constexpr bool SCALED = PD_SCALED_V && !GENERAL_STEP;
     SeedGroup<PD_MODE_WEIGHTED, NP, RESID, GENERAL_STEP> cur;
-    cur.make(at, jbase, pi, i, ivalid, j0, j1, qs_hi, qs_lo, dq_hi, dq_lo);
+    constexpr bool TOP = seeds_at_top_w<K, NP>();
+    if (!TOP) cur.make(at, jbase, pi, i, ivalid, j0, j1, qs_hi, qs_lo, dq_hi, dq_lo);
     for (int j = j0; j < j1; j += NP) {
+        if (TOP) cur.make(at, jbase, pi, i, ivalid, j, j1, qs_hi, qs_lo, dq_hi, dq_lo);
         float2 V[NP], D[NP], NA[NP], WJ[NP], WE[NP], WO[NP], WJE[NP], WJO[NP];
 #pragma unroll
         for (int p = 0; p < NP; ++p) {
@@ -655,7 +681,7 @@ __device__ __forceinline__ void pairs_range_x2w(const float4 *__restrict__ at, i
         }
         const float2 mvs = make_float2(-cur.vsum, -cur.vsum);
         const float2 mvws = make_float2(-cur.vwsum, -cur.vwsum);
-        cur.make(at, jbase, pi, i, ivalid, j + NP, j1, qs_hi, qs_lo, dq_hi, dq_lo);
+        if (!TOP) cur.make(at, jbase, pi, i, ivalid, j + NP, j1, qs_hi, qs_lo, dq_hi, dq_lo);
         int qoff = 0;  // opaque zero: keeps the K/2 q loads in the loop
         if (RESID) asm volatile("mov.b32 %0, %0;" : "+r"(qoff));
 #pragma unroll
@@ -712,8 +738,9 @@ constexpr size_t PD_FP32_DYN_SMEM = 2 * PD_JSTAGE * sizeof(float4);
 // Resident CTAs per SM each FP32 shape is compiled for (register budget
 // 65536 / (128 · blocks) per thread).
 constexpr int fp32_min_blocks(int K, int MODE, int NP) {
-    return MODE == PD_MODE_CLASS ? (K <= 64 ? 4 : (K <= 128 && NP <= 2 ? 3 : 2))
-                                 : (K <= 32 ? 4 : 2);
+    return MODE == PD_MODE_CLASS
+               ? (K <= 64 ? 4 : (K <= 128 && (NP <= 2 || (PD_SEED_TOP && K == 128 && NP == 4)) ? 3 : 2))
+                                 : (K <= 32 ? 4 : (PD_SEED_TOP_W && K == 64 && NP == 2 ? 3 : 2));
 }
 
 // Polls of a bulk-copy wait before it gives up: the normal limit, and the

@@ -179,10 +179,10 @@ Tuning default_tuning(int64_t n_atoms, int64_t nq, int precision, int64_t n_fram
         t.TJ = std::clamp(next_pow2(n_atoms / 16), 256, 4096);
         return t;
     }
-    // Measured on B200 (class mode): K = 128 with 4 pairs per thread (two
-    // CTAs per SM) is the fastest shape from ~4k atoms up — 555.9 ms on the
-    // 100,000-atom solve against 561.5 ms with 2 pairs at three CTAs per SM —
-    // and K = 64 with 4 pairs below; a j chunk of about N/8 atoms balances
+    // Measured on B200 (class mode): K = 128 with 4 pairs per thread (three
+    // CTAs per SM, seeds computed at the top of each pass) is the fastest
+    // shape from ~4k atoms up — 546.7 ms on the 100,000-atom solve against
+    // 561.5 ms with 2 pairs — and K = 64 with 4 pairs below; a j chunk of about N/8 atoms balances
     // tile count against per-tile overhead. The last q-block of a grid runs
     // only the 16-point chunks that lie on it, so a long block wastes at most
     // 15 grid points per request. (These are the shapes of buckets the tuning
