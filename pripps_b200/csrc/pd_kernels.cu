@@ -531,8 +531,12 @@ template <int K, int NP>
 constexpr bool seeds_at_top() {
     return PD_SEED_TOP && K == 128 && NP == 4;
 }
+// The weighted mode's K = 64 with two pairs per thread likewise: 168
+// registers and three CTAs per SM with the seeds at the top of each pass
+// (835 ms on the 100,000-atom solve with per-atom weights, against 857 ms
+// with the next pass's seeds at two CTAs; four pairs: 842 ms).
 #ifndef PD_SEED_TOP_W
-#define PD_SEED_TOP_W 0
+#define PD_SEED_TOP_W 1
 #endif
 template <int K, int NP>
 constexpr bool seeds_at_top_w() {
