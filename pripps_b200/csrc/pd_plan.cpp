@@ -4,7 +4,6 @@
 
 #include <algorithm>
 #include <cmath>
-#include <map>
 #include <numeric>
 #include <utility>
 
@@ -216,6 +215,54 @@ Tuning default_tuning(int64_t n_atoms, int64_t nq, int precision, int64_t n_fram
     return t;
 }
 
+// The distinct (species, weight) keys of the atoms in ascending order and
+// each atom's index among them; false as soon as there are more than
+// max_keys. Weights are finite (validated), so equality is the map order's
+// equivalence. A linear search from the previous atom's key: atoms of one
+// residue or surface patch repeat keys, and there are at most max_keys.
+static bool weight_class_keys(int64_t n, const uint32_t *species, const double *w,
+                              int max_keys, std::vector<std::pair<uint32_t, double>> &keys,
+                              std::vector<int32_t> &atom_key) {
+    std::vector<std::pair<uint32_t, double>> seen;  // first-seen order
+    size_t last = 0;
+    for (int64_t i = 0; i < n; ++i) {
+        const std::pair<uint32_t, double> k(species[i], w[i]);
+        if (seen.empty() || !(seen[last] == k)) {
+            last = std::find(seen.begin(), seen.end(), k) - seen.begin();
+            if (last == seen.size()) {
+                if (static_cast<int>(seen.size()) == max_keys) return false;
+                seen.push_back(k);
+            }
+        }
+        atom_key[i] = static_cast<int32_t>(last);
+    }
+    std::vector<int32_t> order(seen.size()), rank(seen.size());
+    std::iota(order.begin(), order.end(), 0);
+    std::sort(order.begin(), order.end(), [&](int32_t a, int32_t b) { return seen[a] < seen[b]; });
+    keys.resize(seen.size());
+    for (size_t r = 0; r < order.size(); ++r) {
+        rank[order[r]] = static_cast<int32_t>(r);
+        keys[r] = seen[order[r]];
+    }
+    for (int64_t i = 0; i < n; ++i) atom_key[i] = rank[atom_key[i]];
+    return true;
+}
+
+// One key per species present (weight 0), in ascending species order.
+static void species_class_keys(int64_t n, const uint32_t *species, int32_t n_species,
+                               std::vector<std::pair<uint32_t, double>> &keys,
+                               std::vector<int32_t> &atom_key) {
+    std::vector<int32_t> rank(n_species, -1);
+    for (int64_t i = 0; i < n; ++i) rank[species[i]] = 0;
+    keys.clear();
+    for (int32_t sp = 0; sp < n_species; ++sp)
+        if (rank[sp] >= 0) {
+            rank[sp] = static_cast<int32_t>(keys.size());
+            keys.emplace_back(static_cast<uint32_t>(sp), 0.0);
+        }
+    for (int64_t i = 0; i < n; ++i) atom_key[i] = rank[species[i]];
+}
+
 int build_plan(const pd_request *req, const uint32_t *species, const double *w,
                const Tuning &tun, Plan &P, std::string &msg, bool count_pairs) {
     P = Plan();
@@ -244,36 +291,22 @@ int build_plan(const pd_request *req, const uint32_t *species, const double *w,
     P.dq = (P.qmax - P.qmin) / denom;
 
     const int64_t n = P.n_atoms;
-    // ---- classes: species, or (species, weight) while few distinct weights
-    std::map<std::pair<uint32_t, double>, int> keys;
-    bool by_weight = P.has_hyd;
-    if (by_weight) {
-        for (int64_t i = 0; i < n; ++i) {
-            keys.emplace(std::make_pair(species[i], w[i]), 0);
-            if (static_cast<int>(keys.size()) > PD_MAX_CLASSES) {
-                by_weight = false;
-                break;
-            }
-        }
-    }
-    if (!by_weight) {
-        keys.clear();
-        for (int64_t i = 0; i < n; ++i) keys.emplace(std::make_pair(species[i], 0.0), 0);
-    }
+    // ---- classes: species, or (species, weight) while few distinct weights;
+    // numbered in ascending (species, weight) order
+    std::vector<std::pair<uint32_t, double>> keys;
+    std::vector<int32_t> atom_cls(n);
+    const bool by_weight =
+        P.has_hyd && weight_class_keys(n, species, w, PD_MAX_CLASSES, keys, atom_cls);
+    if (!by_weight) species_class_keys(n, species, P.n_species, keys, atom_cls);
     P.mode = (P.has_hyd && !by_weight) ? PD_MODE_WEIGHTED : PD_MODE_CLASS;
     P.nv = P.mode == PD_MODE_WEIGHTED ? 4 : 1;
     P.tun = fit_tuning(P.precision, P.mode, P.tun);
-    int c = 0;
-    for (auto &kv : keys) kv.second = c++;
+    const int c = static_cast<int>(keys.size());
     P.n_cls = c;
     P.cls.assign(c, PdClassDev{});
-    {
-        int ci = 0;
-        for (auto &kv : keys) {
-            P.cls[ci].species = static_cast<int32_t>(kv.first.first);
-            P.cls[ci].w = kv.first.second;
-            ++ci;
-        }
+    for (int ci = 0; ci < c; ++ci) {
+        P.cls[ci].species = static_cast<int32_t>(keys[ci].first);
+        P.cls[ci].w = keys[ci].second;
     }
     // ---- lattice sets: one class each, class mode only
     std::vector<int> lat_of_cls(c, -1);
@@ -305,14 +338,8 @@ int build_plan(const pd_request *req, const uint32_t *species, const double *w,
         lat_of_cls[found] = static_cast<int>(P.lat.size());
         P.lat.push_back(d);
     }
-    std::vector<int32_t> atom_cls(n);
     std::vector<std::vector<int32_t>> members(c);
-    for (int64_t i = 0; i < n; ++i) {
-        const double wk = by_weight ? w[i] : 0.0;
-        const int k = keys.at(std::make_pair(species[i], wk));
-        atom_cls[i] = k;
-        members[k].push_back(static_cast<int32_t>(i));
-    }
+    for (int64_t i = 0; i < n; ++i) members[atom_cls[i]].push_back(static_cast<int32_t>(i));
     // ---- padded layout
     P.cls_start.assign(c, 0);
     int64_t cur = 0;
@@ -499,10 +526,15 @@ int build_plan(const pd_request *req, const uint32_t *species, const double *w,
                     listed[rel[wv]] = true;
                 }
                 if (qb == 0 && count_pairs) {
-                    for (int64_t i = ilo; i < ihi; ++i) {
-                        const int64_t lo = std::max<int64_t>(t.j0, i + 1);
-                        if (t.j1 > lo) covered += static_cast<uint64_t>(t.j1 - lo);
-                    }
+                    // Σ_{i in [ilo, ihi)} max(0, j1 − max(j0, i + 1)): the i
+                    // below j0 − 1 see the whole range, the others an
+                    // arithmetic series j1 − 1 − i
+                    const int64_t j0 = t.j0, j1 = t.j1;
+                    const int64_t a_end = std::min(ihi, j0 - 1);
+                    if (a_end > ilo) covered += static_cast<uint64_t>((a_end - ilo) * (j1 - j0));
+                    const int64_t b0 = std::max(ilo, j0 - 1), b1 = std::min(ihi, j1 - 1);
+                    if (b1 > b0)  // terms j1 − 1 − b0 down to j1 − b1
+                        covered += static_cast<uint64_t>(((j1 - 1 - b0) + (j1 - b1)) * (b1 - b0) / 2);
                 }
             }
             next_slot += nslot;
@@ -522,19 +554,23 @@ int build_plan(const pd_request *req, const uint32_t *species, const double *w,
     for (auto &l : lists) P.lidx.insert(P.lidx.end(), l.begin(), l.end());
 
     // Execution order: longest tiles first (j length), stable; replicated
-    // per frame with frame-offset slots.
-    std::vector<int64_t> order(frame_jobs.size());
+    // per frame with frame-offset slots. A tile's q-block jobs are
+    // consecutive in creation order and of one length, so sorting the tiles
+    // gives the order a stable sort of the jobs would.
+    std::vector<int64_t> order(tiles.size());
     std::iota(order.begin(), order.end(), 0);
     std::stable_sort(order.begin(), order.end(), [&](int64_t x, int64_t y) {
-        return (frame_jobs[x].j1 - frame_jobs[x].j0) > (frame_jobs[y].j1 - frame_jobs[y].j0);
+        return (tiles[x].j1 - tiles[x].j0) > (tiles[y].j1 - tiles[y].j0);
     });
-    P.jobs.reserve(order.size() * P.n_frames);
+    P.jobs.reserve(frame_jobs.size() * P.n_frames);
     for (int64_t o : order) {
-        for (int f = 0; f < P.n_frames; ++f) {
-            PdJob jb = frame_jobs[o];
-            jb.frame = f;
-            jb.slot += static_cast<int64_t>(f) * P.slots_per_frame;
-            P.jobs.push_back(jb);
+        for (int qb = 0; qb < P.nqb; ++qb) {
+            for (int f = 0; f < P.n_frames; ++f) {
+                PdJob jb = frame_jobs[o * P.nqb + qb];
+                jb.frame = f;
+                jb.slot += static_cast<int64_t>(f) * P.slots_per_frame;
+                P.jobs.push_back(jb);
+            }
         }
     }
     return PD_OK;

@@ -1,10 +1,11 @@
 // Kernel-shape tuning table: bucket keys and the tuning file.
 #include "pd_tuning.h"
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <fstream>
-#include <set>
+#include <vector>
 #include <sstream>
 #include <utility>
 
@@ -28,10 +29,17 @@ TuneKey tune_key(int64_t n_atoms, int64_t nq, int precision, int mode, int64_t n
 
 int request_mode(const pd_request *req, const uint32_t *species, const double *weights) {
     if (!req->hyd_weights || !weights) return PD_MODE_CLASS;
-    std::set<std::pair<uint32_t, double>> keys;
+    // distinct (species, weight) keys, searched from the previous atom's
+    std::vector<std::pair<uint32_t, double>> keys;
+    size_t last = 0;
     for (uint64_t i = 0; i < req->n_atoms; ++i) {
-        keys.emplace(species[i], weights[i]);
-        if (static_cast<int>(keys.size()) > PD_MAX_CLASSES) return PD_MODE_WEIGHTED;
+        const std::pair<uint32_t, double> k(species[i], weights[i]);
+        if (!keys.empty() && keys[last] == k) continue;
+        last = std::find(keys.begin(), keys.end(), k) - keys.begin();
+        if (last == keys.size()) {
+            if (static_cast<int>(keys.size()) == PD_MAX_CLASSES) return PD_MODE_WEIGHTED;
+            keys.push_back(k);
+        }
     }
     return PD_MODE_CLASS;
 }
