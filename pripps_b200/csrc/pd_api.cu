@@ -639,6 +639,7 @@ struct PdTicket {
     bool canceled = false;
     bool taken = false;               // result copied out by pd_wait
     size_t next_job = 0;              // first tile not yet issued
+    bool express_wait = false;        // small: waits for a free express lane
     bool finish_issued = false;       // reduction (or, if cancelled, the drain) enqueued
     bool drained_only = false;        // cancelled after admission: no reduction was run
     uint32_t used_streams = 0;        // lane streams that ran some of its tiles
@@ -683,6 +684,15 @@ constexpr double RR_QUANTUM = 1.0e9;   // work a request adds per round-robin tu
 #define PD_EXPRESS_COST 1.0e10
 #endif
 constexpr double EXPRESS_COST = PD_EXPRESS_COST;
+// A small request waits for a free express lane at most this long (s) before
+// it joins the steps. When many arrive at once (a burst admitted in one pass)
+// the four lanes serve them in admission order, a launch of each lane taking
+// every waiting request of its variant that fits, instead of sending the
+// overflow into the round-robin steps beside the large requests.
+#ifndef PD_EXPRESS_MAX_WAIT
+#define PD_EXPRESS_MAX_WAIT 0.25
+#endif
+constexpr double EXPRESS_MAX_WAIT = PD_EXPRESS_MAX_WAIT;
 constexpr int EXPRESS = STEP_BUFS;  // row of the express lanes
 static_assert((STEP_BUFS + 1) * STEP_LANES <= 32, "lane bits of PdTicket::used_streams");
 
@@ -857,7 +867,6 @@ void worker_main(pd_ctx *ctx) {
         nvtxRangePushA("pd admit");
         // ---- admission in FIFO order while the budget allows
         bool admitted_now = false;
-        std::vector<std::shared_ptr<PdTicket>> fresh;  // admitted in this pass
         for (auto &t : head) {
             int rc = t->plan_state < 0 ? t->plan_state : PD_OK;
             if (rc == PD_OK) rc = plan_device(ctx, &t->req, t->dp, sa, /*wait=*/true);
@@ -879,6 +888,17 @@ void worker_main(pd_ctx *ctx) {
                 fail(t, PD_EDEVICE, "pack failed");
                 continue;
             }
+            {
+                // small enough for an express lane?
+                const Plan &P = t->dp.P;
+                double cost = 0;
+                for (const PdJob &jb : P.jobs) {
+                    cost += tile_cost(P, jb);
+                    if (cost > EXPRESS_COST) break;
+                }
+                t->express_wait =
+                    !P.jobs.empty() && cost <= EXPRESS_COST && P.jobs.size() <= STEP_MAX_JOBS;
+            }
             // the device and the pinned image hold the inputs now
             t->xyz = {};
             t->ffA = {};
@@ -890,7 +910,6 @@ void worker_main(pd_ctx *ctx) {
             t->admitted = true;
             t->t_admit = now_s();
             active.push_back(t);
-            fresh.push_back(t);
             admitted_now = true;
         }
         if (admitted_now) {
@@ -900,23 +919,24 @@ void worker_main(pd_ctx *ctx) {
 
         nvtxRangePop();
         nvtxRangePushA("pd express + step");
-        // ---- express: small requests admitted now get all their tiles on a
-        // free express lane of their kernel variant (else they take the steps)
+        // ---- express: small requests, in admission order, get all their
+        // tiles on a free express lane of their kernel variant; one that
+        // finds none waits for the next pass, up to EXPRESS_MAX_WAIT, then
+        // takes the steps
         {
             Lane *ex = lanes[EXPRESS];
             std::tuple<int, int, int, int> ex_key[STEP_LANES];
             std::vector<std::shared_ptr<PdTicket>> ex_members[STEP_LANES];
             size_t ex_nj[STEP_LANES] = {0, 0, 0, 0};
             bool ex_used[STEP_LANES] = {false, false, false, false};
-            for (auto &t : fresh) {
+            const double now = now_s();
+            for (auto &t : active) {
+                if (!t->express_wait) continue;
                 const Plan &P = t->dp.P;
-                if (t->canceled || t->next_job != 0 || P.jobs.empty()) continue;
-                double cost = 0;
-                for (const PdJob &jb : P.jobs) {
-                    cost += tile_cost(P, jb);
-                    if (cost > EXPRESS_COST) break;
+                if (t->canceled || t->next_job != 0) {
+                    t->express_wait = false;
+                    continue;
                 }
-                if (cost > EXPRESS_COST) continue;
                 const auto key = std::make_tuple(P.precision, P.tun.K, P.tun.NP, P.mode);
                 int l = -1;
                 for (int c = 0; c < STEP_LANES && l < 0; ++c)
@@ -934,7 +954,11 @@ void worker_main(pd_ctx *ctx) {
                     ex_key[c] = key;
                     l = c;
                 }
-                if (l < 0) continue;
+                if (l < 0) {
+                    if (now - t->t_admit > EXPRESS_MAX_WAIT) t->express_wait = false;
+                    continue;
+                }
+                t->express_wait = false;
                 const int slot = static_cast<int>(ex_members[l].size());
                 ex_members[l].push_back(t);
                 for (; t->next_job < P.jobs.size(); ++t->next_job) {
@@ -973,7 +997,8 @@ void worker_main(pd_ctx *ctx) {
         // its kernel variant; up to STEP_LANES variants per step.
         std::vector<std::shared_ptr<PdTicket>> cand;
         for (auto &t : active)
-            if (!t->canceled && t->next_job < t->dp.P.jobs.size()) cand.push_back(t);
+            if (!t->canceled && !t->express_wait && t->next_job < t->dp.P.jobs.size())
+                cand.push_back(t);
         Lane *step = lanes[cur];
         std::tuple<int, int, int, int> lane_key[STEP_LANES];
         std::vector<std::shared_ptr<PdTicket>> members[STEP_LANES];
