@@ -352,9 +352,9 @@ def test_serving_alone_equals_mixed(gpu_ctx):
 def test_serving_express_lanes_beside_a_large_request(gpu_ctx):
     """Small requests (at most 1e10 pair·q of work) submitted while a large
     one runs go to the high-priority express lanes at admission: more of them,
-    and of more kernel variants, than there are express lanes (the rest take
-    the steps). Every result equals its solo solve bit for bit, and most small
-    requests finish before the large one."""
+    and of more kernel variants, than there are express lanes (the rest wait
+    for a lane, or after 0.25 s take the steps). Every result equals its solo
+    solve bit for bit, and most small requests finish before the large one."""
     from pripps_b200.serving import Server
     big = workloads.small_globule(30_000, 11, nq=400).request  # ≈1.8e11 pair·q
     small = [workloads.small_globule(n, 20 + k, nq=nq, solvent=sol, precision=prec).request
@@ -374,6 +374,29 @@ def test_serving_express_lanes_beside_a_large_request(gpu_ctx):
         assert np.array_equal(a, b)
     done_big = srv.times(tb)[2]
     assert sum(srv.times(t)[2] < done_big for t in ts) >= len(ts) // 2
+
+
+def test_serving_burst_of_small_requests(gpu_ctx):
+    """Eighty small requests of four kernel variants and two large ones
+    submitted at once (one admission pass): the small ones queue for the
+    express lanes, each lane launch taking every waiting request of its
+    variant. Every result equals its solo solve bit for bit, and the small
+    requests finish before the large ones."""
+    from pripps_b200.serving import Server
+    rng = np.random.default_rng(3)
+    specs = [(int(rng.integers(300, 2500)), int(rng.integers(30, 400)), bool(k % 3),
+              "fp64" if k % 10 == 0 else "fp32") for k in range(80)]
+    small = [workloads.small_globule(n, 100 + k, nq=nq, solvent=sol, precision=prec).request
+             for k, (n, nq, sol, prec) in enumerate(specs)]
+    big = [workloads.small_globule(25_000, 7 + k, nq=300).request for k in range(2)]
+    solo = [solve(r, gpu_ctx) for r in small + big]
+    srv = Server(gpu_ctx)
+    tickets = [srv.submit(r) for r in big + small]
+    outs = [srv.wait(t, timeout_s=180) for t in tickets]
+    for a, b in zip(outs, solo[-2:] + solo[:-2]):
+        assert np.array_equal(a, b)
+    done_big = min(srv.times(t)[2] for t in tickets[:2])
+    assert sum(srv.times(t)[2] < done_big for t in tickets[2:]) >= 70
 
 
 def test_serving_budget_admission(gpu_ctx):
