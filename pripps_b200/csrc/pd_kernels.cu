@@ -516,31 +516,28 @@ __device__ __forceinline__ void pairs_range(const float4 *__restrict__ at, int j
 #ifndef PD_SCALED_V
 #define PD_SCALED_V 1
 #endif
-// Where the seeds of a pass are computed. With K = 128 and four pairs per
-// thread each pass computes its own seeds before its steps: no next-pass
-// seeds are held through the steps, the kernel fits 168 registers and three
-// CTAs per SM instead of 255 and two, and the third warp per scheduler hides
-// the seeds' dependency chains (546.7 ms against 556.0 ms on the
-// 100,000-atom solve; with two CTAs per SM seeds at the top measured
-// 558.5 ms). Every other shape computes the next pass's seeds while the
-// current pass steps (it gains no CTA from the registers freed).
+// Where the seeds of a pass are computed. Computing each pass's seeds
+// before its steps holds no next-pass seeds through the steps: fewer
+// registers, so more resident CTAs or fewer spills, and the extra warps per
+// scheduler hide the seeds' dependency chains. Measured on B200 (pair-kernel
+// time): K = 128 with four pairs per thread fits 168 registers and three CTAs
+// per SM instead of 255 and two, 546.7 ms against 556.0 ms on the
+// 100,000-atom solve (558.5 ms with the seeds at the top but two CTAs); K = 64
+// with four pairs loses its spills at four CTAs, 0.216 against 0.232 ms on
+// 3,000 atoms at nq 300; the weighted mode's K = 64 fits three CTAs instead of
+// two, 814 against 842 ms on the 100,000-atom solve with per-atom weights.
+// The other shapes compute the next pass's seeds while the current pass
+// steps (K = 128 with two pairs: 3.117 against 3.121 ms on 10,000 atoms).
 #ifndef PD_SEED_TOP
 #define PD_SEED_TOP 1
 #endif
 template <int K, int NP>
 constexpr bool seeds_at_top() {
-    return PD_SEED_TOP && K == 128 && NP == 4;
+    return PD_SEED_TOP && (K == 64 || (K == 128 && NP == 4));
 }
-// The weighted mode's K = 64 with two pairs per thread likewise: 168
-// registers and three CTAs per SM with the seeds at the top of each pass
-// (835 ms on the 100,000-atom solve with per-atom weights, against 857 ms
-// with the next pass's seeds at two CTAs; four pairs: 842 ms).
-#ifndef PD_SEED_TOP_W
-#define PD_SEED_TOP_W 1
-#endif
 template <int K, int NP>
 constexpr bool seeds_at_top_w() {
-    return PD_SEED_TOP_W && K == 64 && NP == 2;
+    return PD_SEED_TOP && K == 64;
 }
 // Instruction order within a step: 0 = d-steps, accumulations, v-steps;
 // 1 = d-steps, then per pair its accumulation and v-step; 2 (with
@@ -744,7 +741,7 @@ constexpr size_t PD_FP32_DYN_SMEM = 2 * PD_JSTAGE * sizeof(float4);
 constexpr int fp32_min_blocks(int K, int MODE, int NP) {
     return MODE == PD_MODE_CLASS
                ? (K <= 64 ? 4 : (K <= 128 && (NP <= 2 || (PD_SEED_TOP && K == 128 && NP == 4)) ? 3 : 2))
-                                 : (K <= 32 ? 4 : (PD_SEED_TOP_W && K == 64 && NP == 2 ? 3 : 2));
+               : (K <= 32 ? 4 : (PD_SEED_TOP && K == 64 ? 3 : 2));
 }
 
 // Polls of a bulk-copy wait before it gives up: the normal limit, and the

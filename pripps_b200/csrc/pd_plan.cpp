@@ -154,8 +154,8 @@ static int next_pow2(int64_t v) {
 
 Tuning fit_tuning(int precision, int mode, Tuning t) {
     // Two accumulators per q (weighted mode) allow q blocks up to 64 (there
-    // four pairs per thread measured fastest: 842 ms on the 100,000-atom solve
-    // with per-atom hydration weights against 857 ms with two); FP64 runs one
+    // four pairs per thread measured fastest: 814 ms on the 100,000-atom solve
+    // with per-atom hydration weights against 835 ms with two); FP64 runs one
     // pair per pass.
     if (precision == PD_FP64) {
         t.NP = 1;
