@@ -562,16 +562,18 @@ def timed_workload(ctx, w, local, min_seconds=2.0):
 
 def serving_burst(ctx, local, n_requests=400, precision="fp32"):
     """n_requests requests of the serving stream's distribution submitted at
-    once to the request loop: p50/p99 latency and aggregate pair·q/s."""
+    once to the request loop, after the same burst once untimed: p50/p99
+    latency and aggregate pair·q/s."""
     from pripps_b200 import synth, workloads
     from pripps_b200.serving import Server
     stream = synth.request_stream(n_requests, 1e9, seed=4)
     pool = workloads.GlobulePool()
     reqs = [workloads.stream_request_pooled(sr, pool, precision) for sr in stream]
     srv = Server(ctx)
-    # warm the loop's lanes and captured graphs for the kernel variants the
-    # burst uses: its first 100 requests at once, untimed
-    for t in [srv.submit(w.request) for w in reqs[:100]]:
+    # warm the loop (lanes and captured graphs of the kernel variants the
+    # burst uses, the device pool and the pinned staging blocks grown to the
+    # burst's concurrency): the same burst once, untimed
+    for t in [srv.submit(w.request) for w in reqs]:
         srv.wait(t)
     clocks = ClockSampler(local)
     clocks.start()
