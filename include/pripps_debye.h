@@ -359,7 +359,8 @@ const char *pd_last_error(pd_ctx *ctx);
  * pd_autotune_request times every candidate shape on the caller's own
  * request (its structure, solvent model and grid; no lattice sets), each
  * timed execution after an L2 flush, stores the fastest for the request's
- * bucket and returns it with its time; pd_autotune does the same on a
+ * bucket (of the shapes within 0.3 % of the fastest time, the one that holds
+ * the least device memory) and returns it with its time; pd_autotune does the same on a
  * synthetic solvent globule of n_atoms atoms (class mode, one frame). Both
  * run on the context's stream: do not overlap them with other work on the
  * context. pd_get_tuning / pd_set_tuning read and write the class-mode,
@@ -436,12 +437,13 @@ uint64_t pd_launch_count(pd_ctx *ctx);
  *    partial sums) needs more than PD_NOALLOC_SCRATCH_BYTES fails with
  *    PD_EBUDGET and a message naming both sizes, before any device work.
  *    pd_request_device_bytes(ctx, req, 0, &bytes) gives a request's need
- *    beforehand; the need depends on the atom classes as well as on N and
+ *    beforehand; the need depends on the atom classes and on the j chunk
+ *    the tuning table picks for the request's bucket as well as on N and
  *    nq. As a guide, at nq = 1,000 an FP32 solve with solvent and one
- *    hydration weight per element fits up to about 100,000 atoms (the
- *    100,000-atom ellipsoid needs 59 MB, 110,000 atoms of it 71 MB) and
- *    200,000 atoms are refused; with a hydration weight per atom (four
- *    partial sums per grid point) the limit is about 60,000 atoms.
+ *    hydration weight per element fits up to roughly 130,000 atoms (the
+ *    100,000-atom ellipsoid needs 49 MB) and 200,000 atoms are refused;
+ *    with a hydration weight per atom (four partial sums per grid point)
+ *    up to about 20,000 atoms fit, and larger requests may not.
  *  - The array occupies PD_NOALLOC_SCRATCH_BYTES of memory on every GPU that
  *    loads the library's device code, until the process exits.
  *  - Every call shares the array, which keeps the previous call's contents;

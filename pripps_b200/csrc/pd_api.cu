@@ -1750,9 +1750,9 @@ std::vector<Tuning> tune_candidates(const pd_request *req, int mode) {
     else
         shapes = {{64, 2}, {64, 4}, {96, 2}, {128, 1}, {128, 2}, {128, 4}};
     std::vector<int> tjs;
-    for (int d : {32, 16, 8, 4}) {
+    for (int d : {32, 16, 8, 4, 2}) {
         int tj = 256;
-        while (tj < n / d && tj < 16384) tj <<= 1;
+        while (tj < n / d && tj < 65536) tj <<= 1;
         if (std::find(tjs.begin(), tjs.end(), tj) == tjs.end()) tjs.push_back(tj);
     }
     std::vector<Tuning> out;
@@ -1809,11 +1809,12 @@ int autotune_request(pd_ctx *ctx, const pd_request *req, Tuning *best_out, doubl
     if (e == cudaSuccess) e = cudaEventCreate(&e0);
     if (e == cudaSuccess) e = cudaEventCreate(&e1);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    double best = 1e300;
-    Tuning best_t = cands.front();
+    // measured time and device bytes of every candidate that ran
+    std::vector<std::pair<double, uint64_t>> measured(cands.size(), {1e300, 0});
     for (size_t c = 0; c < cands.size() && e == cudaSuccess; ++c) {
         pd_plan *plan = nullptr;
         if (plan_create_impl(ctx, req, &plan, &cands[c]) != PD_OK) continue;
+        const uint64_t bytes = plan->dp.L.total;
         // warm-up, then timed executions (one when a run takes over 0.25 s)
         bool ok = pd_plan_execute(ctx, plan, xyz_dev, out_dev, st) == PD_OK;
         double total = 0.0;
@@ -1831,11 +1832,27 @@ int autotune_request(pd_ctx *ctx, const pd_request *req, Tuning *best_out, doubl
             if (ms > 250.0f && reps >= 1) break;
         }
         pd_plan_destroy(ctx, plan);
-        if (ok && reps > 0 && total / reps < best) {
-            best = total / reps;
+        if (ok && reps > 0) measured[c] = {total / reps, bytes};
+    }
+    // The fastest shape; among shapes within TUNE_TIE of its time the one
+    // that holds the least device memory (a longer j chunk means fewer tiles
+    // and FP64 tile slots at the same speed).
+    constexpr double TUNE_TIE = 0.003;
+    double best = 1e300;
+    for (const auto &m : measured) best = std::min(best, m.first);
+    Tuning best_t = cands.front();
+    double pick_ms = 1e300;
+    uint64_t pick_bytes = ~uint64_t{0};
+    for (size_t c = 0; c < cands.size() && best < 1e300; ++c) {
+        const auto &m = measured[c];
+        if (m.first > best * (1.0 + TUNE_TIE)) continue;
+        if (m.second < pick_bytes || (m.second == pick_bytes && m.first < pick_ms)) {
             best_t = cands[c];
+            pick_ms = m.first;
+            pick_bytes = m.second;
         }
     }
+    if (best < 1e300) best = pick_ms;
     if (xyz_dev) cudaFreeAsync(xyz_dev, st);
     if (out_dev) cudaFreeAsync(out_dev, st);
     if (flush) cudaFreeAsync(flush, st);

@@ -15,6 +15,7 @@ This file sorts last so that a run stopping at its first failure has run
 every other test before it.
 """
 import ctypes as C
+import os
 
 import numpy as np
 import pytest
@@ -125,8 +126,11 @@ def test_noalloc_refuses_requests_beyond_the_scratch():
 def test_noalloc_size_guide_holds():
     """Host-only: the header's guide — at nq = 1,000 an FP32 solve of 100,000
     atoms with solvent and one hydration weight per element fits the fixed
-    scratch and 200,000 atoms do not; with a weight per atom 60,000 atoms fit
-    and 70,000 do not — checked on the layout the entry point computes."""
+    scratch and 200,000 atoms do not; with a weight per atom 20,000 atoms fit
+    and 70,000 do not — checked on the layout the entry point computes with
+    the shipped tuning table."""
+    if os.environ.get("PRIPPS_DEBYE_TUNING"):
+        pytest.skip("a tuning file other than the shipped one is in use")
     def need(n, nq, per_atom_weights=False):
         rng = np.random.default_rng(n)
         w = np.where(rng.random(n) < 0.3, 1.2, 0.0)
@@ -142,7 +146,7 @@ def test_noalloc_size_guide_holds():
         return out.value
     assert need(100_000, 1000) <= _lib.PD_NOALLOC_SCRATCH_BYTES
     assert need(200_000, 1000) > _lib.PD_NOALLOC_SCRATCH_BYTES
-    assert need(60_000, 1000, True) <= _lib.PD_NOALLOC_SCRATCH_BYTES
+    assert need(20_000, 1000, True) <= _lib.PD_NOALLOC_SCRATCH_BYTES
     assert need(70_000, 1000, True) > _lib.PD_NOALLOC_SCRATCH_BYTES
 
 
