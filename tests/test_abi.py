@@ -80,6 +80,29 @@ def test_plan_covers_pairs_for_workload_shapes():
     assert ncls == 8  # 4 species × {buried, exposed}
 
 
+@pytest.mark.parametrize("n_keys", [1, 47, 48, 49, 200])
+def test_atom_classes_follow_the_key_count(n_keys):
+    """Classes are the distinct (species, hydration weight) keys while there
+    are at most 48 of them, else the species present (weighted mode); -0.0
+    and 0.0 are one weight."""
+    rng = np.random.default_rng(n_keys)
+    n = 3000
+    req = _req(n=n, solvent=True, weights_mode="class")
+    sp = rng.integers(0, 4, n).astype(np.uint32)
+    keys = [(int(k % 4), 0.25 * (k // 4)) for k in range(n_keys)]
+    pick = rng.integers(0, n_keys, n)
+    pick[:n_keys] = np.arange(n_keys)  # every key present
+    sp = np.array([keys[k][0] for k in pick], dtype=np.uint32)
+    w = np.array([keys[k][1] for k in pick])
+    w[(w == 0.0) & (rng.random(n) < 0.5)] = -0.0
+    req.species, req.hyd_weights = sp, w
+    rc, (ncls, npad, ntiles, covered) = inspect(req)
+    assert rc == 0, _lib.last_error()
+    assert covered == n * (n - 1) // 2
+    expect = len(set(keys)) if len(set(keys)) <= 48 else len(set(sp.tolist()))
+    assert ncls == expect
+
+
 def test_validation_errors_before_any_device_work():
     base = _req(n=10, nq=5)
     bad = []
