@@ -294,6 +294,8 @@ def run_ours(args, ws, rank, local):
         ends[i].record(stream)
         flush.zero_()
     torch.cuda.synchronize()
+    if ws > 1:
+        torch.distributed.barrier()
     launches = ctx.launch_count() - launches0
     clk = clocks.stop()
     step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
